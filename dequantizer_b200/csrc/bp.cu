@@ -1,0 +1,226 @@
+// Belief-propagation kernels (FP64 / complex128, generic shapes).
+//
+// Node update, replacing dequantizer/src/tensor_ops.py:36-60
+// (pass_through_node) inside the sweep of mappings/belief_propagation.py:24-64.
+// One CTA owns one half-edge h = (node v, bond e). It walks the bond-e slices
+// T[.., a_e = a, ..] of the node tensor, contracts each slice with the k-1
+// incoming messages (mode products in shared memory or CTA scratch), and
+// accumulates column a of the outgoing message,
+//     m_out[a', a] = sum_x conj(T_slice(a')[x]) Y_a[x],
+// then divides by the trace.
+//
+// The incoming message of every bond is chosen per half-edge (src_sel), which
+// reproduces the reference's synchronous sweep (all DQZ_SRC_E2N_OLD), its
+// asynchronous sweep in traversal order (a mix, with nodes launched level by
+// level) and a flooding schedule (all DQZ_SRC_N2E_OLD).
+#include "common.cuh"
+
+using namespace dqz;
+
+namespace {
+
+constexpr int BP_THREADS = 256;
+
+__device__ __forceinline__ const cd *incoming_msg(const dqz_graph_t &g, int hf, const cd *n2e_old, const cd *e2n_old,
+                                                  const cd *n2e_new, const uint8_t *src_sel) {
+  int sel = src_sel[hf];
+  if (sel == DQZ_SRC_E2N_OLD) return e2n_old + g.half_msg_off[hf];
+  int tw = g.half_twin[hf];
+  return (sel == DQZ_SRC_N2E_NEW ? n2e_new : n2e_old) + g.half_msg_off[tw];
+}
+
+__global__ void __launch_bounds__(BP_THREADS) bp_node_generic(dqz_graph_t g, const cd *__restrict__ T,
+                                                              const cd *n2e_old, const cd *e2n_old, cd *n2e_new,
+                                                              const uint8_t *__restrict__ src_sel,
+                                                              const int32_t *__restrict__ halves, int n_halves,
+                                                              int max_slice, int max_chi, cd *scratch) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cd *out = reinterpret_cast<cd *>(smem_raw + 48 * sizeof(double));  // max_chi^2
+  cd *bufA, *bufB;
+  if (scratch) {
+    bufA = scratch + (long long)blockIdx.x * 2 * max_slice;
+  } else {
+    bufA = out + (long long)max_chi * max_chi;
+  }
+  bufB = bufA + max_slice;
+  __shared__ cd trace_sh;
+
+  for (int item = blockIdx.x; item < n_halves; item += gridDim.x) {
+    const int h = halves[item];
+    const int v = g.half_node[h];
+    NodeShape s;
+    load_shape(g, v, s);
+    const int e = h - s.half0;
+    const int ce = s.dims[e];
+    const cd *Tv = T + g.node_off[v];
+    const long long Re = s.stride[e];
+    const long long P = s.size / ce;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+
+    for (int a = 0; a < ce; ++a) {
+      for (long long x = threadIdx.x; x < P; x += blockDim.x) {
+        long long l = x / Re, r = x - l * Re;
+        bufA[x] = Tv[(l * ce + a) * Re + r];
+      }
+      __syncthreads();
+      cd *cur = bufA, *nxt = bufB;
+      long long Lj = 1;
+      for (int f = 0; f < s.k; ++f) {
+        if (f == e) continue;
+        const int q = s.dims[f];
+        const long long R = P / Lj / q;
+        const cd *m = incoming_msg(g, s.half0 + f, n2e_old, e2n_old, n2e_new, src_sel);
+        mode_product<false>(cur, nxt, Lj, q, q, R, m, q, 1);
+        __syncthreads();
+        cd *t = cur;
+        cur = nxt;
+        nxt = t;
+        Lj *= q;
+      }
+      for (int ap = warp; ap < ce; ap += nw) {
+        cd acc = czero();
+        for (long long x = lane; x < P; x += 32) {
+          long long l = x / Re, r = x - l * Re;
+          cfmac(acc, Tv[(l * ce + ap) * Re + r], cur[x]);
+        }
+        acc = warp_csum(acc);
+        if (lane == 0) out[ap * ce + a] = acc;
+      }
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+      cd tr = czero();
+      for (int i = 0; i < ce; ++i) tr = cadd(tr, out[i * ce + i]);
+      trace_sh = tr;
+    }
+    __syncthreads();
+    const cd tr = trace_sh;
+    cd *dst = n2e_new + g.half_msg_off[h];
+    for (int i = threadIdx.x; i < ce * ce; i += blockDim.x) dst[i] = cdiv(out[i], tr);
+    __syncthreads();
+  }
+}
+
+__global__ void bp_edge_pass_kernel(dqz_graph_t g, const cd *n2e_old, const cd *n2e_new,
+                                    const uint8_t *__restrict__ edge_new, cd *e2n_new) {
+  const int nh = g.n_halves;
+  // one warp per half-edge
+  const int warps_per_block = blockDim.x >> 5;
+  const int lane = threadIdx.x & 31;
+  for (int h = blockIdx.x * warps_per_block + (threadIdx.x >> 5); h < nh; h += gridDim.x * warps_per_block) {
+    const int e = g.half_edge[h];
+    const int tw = g.half_twin[h];
+    if (e < 0 || tw < 0) continue;
+    const int c = g.edge_chi[e];
+    const cd *src = (edge_new[h] ? n2e_new : n2e_old) + g.half_msg_off[tw];
+    cd *dst = e2n_new + g.half_msg_off[h];
+    for (int i = lane; i < c * c; i += 32) dst[i] = src[i];
+  }
+}
+
+// partial[h] = |n2e_a[h] - n2e_b[h]|_F, partial[2E + h] = |e2n_a[h] - e2n_b[h]|_F
+__global__ void msg_dist_kernel(dqz_graph_t g, const cd *n2e_a, const cd *n2e_b, const cd *e2n_a, const cd *e2n_b,
+                                double *partial) {
+  const int nh = g.n_halves;
+  const int wpb = blockDim.x >> 5;
+  const int lane = threadIdx.x & 31;
+  for (int w = blockIdx.x * wpb + (threadIdx.x >> 5); w < 2 * nh; w += gridDim.x * wpb) {
+    const int h = w < nh ? w : w - nh;
+    const cd *A = (w < nh ? n2e_a : e2n_a) + g.half_msg_off[h];
+    const cd *B = (w < nh ? n2e_b : e2n_b) + g.half_msg_off[h];
+    const int e = g.half_edge[h];
+    if (e < 0) {
+      if (lane == 0) partial[w] = 0.0;
+      continue;
+    }
+    const int c = g.edge_chi[e];
+    double acc = 0.0;
+    for (int i = lane; i < c * c; i += 32) acc += cabs2(csub(A[i], B[i]));
+    acc = warp_sum(acc);
+    if (lane == 0) partial[w] = sqrt(acc);
+  }
+}
+
+// out[0] = sum(partial[0..n)) * scale, deterministic single-CTA reduction.
+__global__ void reduce_sum_kernel(const double *partial, int n, double scale, double *out) {
+  __shared__ double red[48];
+  double acc = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) acc += partial[i];
+  acc = block_sum(acc, red);
+  if (threadIdx.x == 0) out[0] = acc * scale;
+}
+
+size_t bp_smem_bytes(int max_slice, int max_chi, bool use_scratch) {
+  size_t b = 48 * sizeof(double) + (size_t)max_chi * max_chi * sizeof(cd);
+  if (!use_scratch) b += 2 * (size_t)max_slice * sizeof(cd);
+  return b;
+}
+
+constexpr size_t BP_SMEM_LIMIT = 200 * 1024;
+constexpr int BP_SCRATCH_GRID = 148 * 4;
+
+}  // namespace
+
+extern "C" size_t dqz_bp_node_scratch_bytes(int32_t n_halves, int32_t max_slice, int32_t max_chi) {
+  if (bp_smem_bytes(max_slice, max_chi, false) <= BP_SMEM_LIMIT) return 0;
+  int grid = n_halves < BP_SCRATCH_GRID ? n_halves : BP_SCRATCH_GRID;
+  return (size_t)grid * 2 * (size_t)max_slice * sizeof(cd);
+}
+
+extern "C" int dqz_bp_node_update(const dqz_graph_t *g, const void *tensors, const void *n2e_old,
+                                  const void *e2n_old, void *n2e_new, const uint8_t *src_sel,
+                                  const int32_t *halves, int32_t n_halves, int32_t max_slice, int32_t max_chi,
+                                  void *scratch, cudaStream_t stream) {
+  if (!g || !tensors || !n2e_new || !src_sel || !halves || n_halves < 0 || max_slice <= 0) return DQZ_ERR_ARG;
+  if (max_chi <= 0 || max_chi > DQZ_MAX_CHI) return DQZ_ERR_UNSUPPORTED;
+  if (n_halves == 0) return DQZ_OK;
+  const bool use_scratch = bp_smem_bytes(max_slice, max_chi, false) > BP_SMEM_LIMIT;
+  if (use_scratch && !scratch) return DQZ_ERR_ARG;
+  const size_t smem = bp_smem_bytes(max_slice, max_chi, use_scratch);
+  if (smem > BP_SMEM_LIMIT) return DQZ_ERR_UNSUPPORTED;
+  cudaFuncSetAttribute(bp_node_generic, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)BP_SMEM_LIMIT);
+  int grid = use_scratch ? (n_halves < BP_SCRATCH_GRID ? n_halves : BP_SCRATCH_GRID) : n_halves;
+  bp_node_generic<<<grid, BP_THREADS, smem, stream>>>(
+      *g, (const cd *)tensors, (const cd *)n2e_old, (const cd *)e2n_old, (cd *)n2e_new, src_sel, halves, n_halves,
+      max_slice, max_chi, use_scratch ? (cd *)scratch : nullptr);
+  DQZ_CHECK_LAUNCH();
+  return DQZ_OK;
+}
+
+extern "C" int dqz_bp_edge_pass(const dqz_graph_t *g, const void *n2e_old, const void *n2e_new,
+                                const uint8_t *edge_new, void *e2n_new, int32_t max_chi, cudaStream_t stream) {
+  if (!g || !n2e_old || !n2e_new || !edge_new || !e2n_new) return DQZ_ERR_ARG;
+  if (max_chi <= 0 || max_chi > DQZ_MAX_CHI) return DQZ_ERR_UNSUPPORTED;
+  const int nh = g->n_halves;
+  if (nh == 0) return DQZ_OK;
+  const int wpb = 8;
+  int grid = (nh + wpb - 1) / wpb;
+  bp_edge_pass_kernel<<<grid, wpb * 32, 0, stream>>>(*g, (const cd *)n2e_old, (const cd *)n2e_new, edge_new,
+                                                    (cd *)e2n_new);
+  DQZ_CHECK_LAUNCH();
+  return DQZ_OK;
+}
+
+extern "C" int dqz_messages_distance(const dqz_graph_t *g, const void *n2e_a, const void *n2e_b, const void *e2n_a,
+                                     const void *e2n_b, double *partial, double *out, int32_t max_chi,
+                                     cudaStream_t stream) {
+  if (!g || !n2e_a || !n2e_b || !e2n_a || !e2n_b || !partial || !out) return DQZ_ERR_ARG;
+  if (max_chi <= 0 || max_chi > DQZ_MAX_CHI) return DQZ_ERR_UNSUPPORTED;
+  const int nh = g->n_halves;
+  if (nh == 0) return DQZ_ERR_ARG;
+  const int wpb = 8;
+  int grid = (2 * nh + wpb - 1) / wpb;
+  msg_dist_kernel<<<grid, wpb * 32, 0, stream>>>(*g, (const cd *)n2e_a, (const cd *)n2e_b, (const cd *)e2n_a,
+                                                (const cd *)e2n_b, partial);
+  DQZ_CHECK_LAUNCH();
+  reduce_sum_kernel<<<1, 256, 0, stream>>>(partial, 2 * nh, 1.0 / (2.0 * nh), out);
+  DQZ_CHECK_LAUNCH();
+  return DQZ_OK;
+}
+
+extern "C" int dqz_reduce_sum(const double *partial, int32_t n, double scale, double *out, cudaStream_t stream) {
+  if (!partial || !out || n <= 0) return DQZ_ERR_ARG;
+  reduce_sum_kernel<<<1, 256, 0, stream>>>(partial, n, scale, out);
+  DQZ_CHECK_LAUNCH();
+  return DQZ_OK;
+}

@@ -1,0 +1,130 @@
+// Shared device helpers for libdqz: complex arithmetic on interleaved
+// (re, im) pairs, CTA-wide reductions, and decoding of node-tensor shapes
+// from the packed graph tables.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <math.h>
+
+#include "../../include/dqz.h"
+
+namespace dqz {
+
+// ---------------------------------------------------------------- complex
+typedef double2 cd;  // complex128 as (re, im)
+
+__host__ __device__ __forceinline__ cd mk(double r, double i) { return make_double2(r, i); }
+__host__ __device__ __forceinline__ cd czero() { return make_double2(0.0, 0.0); }
+__host__ __device__ __forceinline__ cd cadd(cd a, cd b) { return mk(a.x + b.x, a.y + b.y); }
+__host__ __device__ __forceinline__ cd csub(cd a, cd b) { return mk(a.x - b.x, a.y - b.y); }
+__host__ __device__ __forceinline__ cd cmul(cd a, cd b) { return mk(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
+// conj(a) * b
+__host__ __device__ __forceinline__ cd cmulc(cd a, cd b) { return mk(a.x * b.x + a.y * b.y, a.x * b.y - a.y * b.x); }
+__host__ __device__ __forceinline__ cd cconj(cd a) { return mk(a.x, -a.y); }
+__host__ __device__ __forceinline__ cd cscale(cd a, double s) { return mk(a.x * s, a.y * s); }
+__host__ __device__ __forceinline__ double cabs2(cd a) { return a.x * a.x + a.y * a.y; }
+// acc += a * b
+__device__ __forceinline__ void cfma(cd &acc, cd a, cd b) {
+  acc.x = fma(a.x, b.x, acc.x);
+  acc.x = fma(-a.y, b.y, acc.x);
+  acc.y = fma(a.x, b.y, acc.y);
+  acc.y = fma(a.y, b.x, acc.y);
+}
+// acc += conj(a) * b
+__device__ __forceinline__ void cfmac(cd &acc, cd a, cd b) {
+  acc.x = fma(a.x, b.x, acc.x);
+  acc.x = fma(a.y, b.y, acc.x);
+  acc.y = fma(a.x, b.y, acc.y);
+  acc.y = fma(-a.y, b.x, acc.y);
+}
+__device__ __forceinline__ cd cdiv(cd a, cd b) {
+  double den = b.x * b.x + b.y * b.y;
+  return mk((a.x * b.x + a.y * b.y) / den, (a.y * b.x - a.x * b.y) / den);
+}
+
+// ------------------------------------------------------------- reductions
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ cd warp_csum(cd v) {
+  v.x = warp_sum(v.x);
+  v.y = warp_sum(v.y);
+  return v;
+}
+
+// Sum over the CTA; every thread gets the result. `red` needs 33 doubles of
+// shared memory. Contains __syncthreads, so all threads must call it.
+__device__ __forceinline__ double block_sum(double v, double *red) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int nw = (blockDim.x + 31) >> 5;
+  v = warp_sum(v);
+  __syncthreads();
+  if (lane == 0) red[warp] = v;
+  __syncthreads();
+  if (warp == 0) {
+    double t = lane < nw ? red[lane] : 0.0;
+    t = warp_sum(t);
+    if (lane == 0) red[32] = t;
+  }
+  __syncthreads();
+  return red[32];
+}
+
+// --------------------------------------------------------------- shapes
+struct NodeShape {
+  int k;            // degree
+  int d;            // physical dimension
+  int half0;        // first half-edge
+  int dims[DQZ_MAX_DEGREE];
+  long long stride[DQZ_MAX_DEGREE];  // element strides of the bonds
+  long long size;   // d * prod dims
+};
+
+__device__ __forceinline__ void load_shape(const dqz_graph_t &g, int v, NodeShape &s) {
+  s.k = g.node_degree[v];
+  s.d = g.node_phys[v];
+  s.half0 = g.node_half[v];
+  long long st = s.d;
+  for (int j = s.k - 1; j >= 0; --j) {
+    int e = g.half_edge[s.half0 + j];
+    s.dims[j] = g.edge_chi[e];
+    s.stride[j] = st;
+    st *= s.dims[j];
+  }
+  s.size = st;
+}
+
+// Generic CTA-cooperative mode product on a row-major tensor:
+//   Y[l, i, r] = sum_b M(i, b) X[l, b, r],  M(i, b) = m[i * rs + b * cs] (optionally conj)
+// X has shape (L, qin, R); Y has shape (L, qout, R). X and Y must not alias.
+template <bool CONJ>
+__device__ __forceinline__ void mode_product(const cd *__restrict__ X, cd *__restrict__ Y, long long L, int qin,
+                                             int qout, long long R, const cd *__restrict__ m, int rs, int cs) {
+  const long long total = L * qout * R;
+  for (long long o = threadIdx.x; o < total; o += blockDim.x) {
+    long long r = o % R;
+    long long t = o / R;
+    int i = (int)(t % qout);
+    long long l = t / qout;
+    const cd *x = X + (l * qin) * R + r;
+    const cd *mm = m + (long long)i * rs;
+    cd acc = czero();
+    for (int b = 0; b < qin; ++b) {
+      cd mv = mm[(long long)b * cs];
+      if (CONJ) mv = cconj(mv);
+      cfma(acc, mv, x[(long long)b * R]);
+    }
+    Y[o] = acc;
+  }
+}
+
+}  // namespace dqz
+
+#define DQZ_CHECK_LAUNCH()                                    \
+  do {                                                        \
+    cudaError_t _e = cudaGetLastError();                      \
+    if (_e != cudaSuccess) return DQZ_ERR_CUDA;               \
+  } while (0)

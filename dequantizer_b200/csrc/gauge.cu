@@ -1,0 +1,458 @@
+// Gauge kernels (FP64 / complex128):
+//  * vidal_edges    -- tensor_ops.py:108-130 (edge_svd), one CTA per edge
+//  * absorb         -- tensor_ops.py:88-93 (absorb_by_node), one CTA per node
+//  * vidal_distance -- tensor_ops.py:143-175 + mappings/vidal_distance.py:17-42
+//  * symmetric      -- tensor_ops.py:189-199 (canonicalize)
+//  * lambdas->msgs  -- mappings/symmetric_gauge.py:50-61
+//  * density        -- mappings/density_matrix.py:16-37
+#include "linalg.cuh"
+
+using namespace dqz;
+
+namespace {
+
+constexpr int GAUGE_THREADS = 256;
+constexpr size_t SMEM_LIMIT = 200 * 1024;
+constexpr int SCRATCH_GRID = 148 * 4;
+const double F32_MAX = 3.4028234663852886e38;
+
+__device__ __forceinline__ double safe_inverse(double l, double eps) { return 1.0 / ((l < eps ? F32_MAX : 0.0) + l); }
+__device__ __forceinline__ double safe_truncate(double l, double eps) { return l > eps ? l : 0.0; }
+
+// ----------------------------------------------------------- vidal edges
+// Work buffers per edge (each chi^2 complex): Af Vf Ab Vb Qf Qb C W, plus
+// wf wb s (chi doubles each), perm/acc ints.
+__host__ __device__ inline size_t vidal_edge_bytes(int c) {
+  return 8 * (size_t)c * c * sizeof(cd) + 3 * (size_t)c * sizeof(double) + 2 * (size_t)c * sizeof(int) + 64;
+}
+
+__global__ void __launch_bounds__(GAUGE_THREADS) vidal_edges_kernel(dqz_graph_t g, const cd *__restrict__ n2e,
+                                                                     double eps, cd *orth, double *lambdas,
+                                                                     int max_chi, unsigned char *scratch) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double *red = reinterpret_cast<double *>(smem_raw);
+  Rot *rots = reinterpret_cast<Rot *>(smem_raw + 48 * sizeof(double));
+  int *flag = reinterpret_cast<int *>(rots + (DQZ_MAX_CHI / 2 + 1));
+  unsigned char *base = reinterpret_cast<unsigned char *>(flag + 4);
+  if (scratch) base = scratch + (size_t)blockIdx.x * vidal_edge_bytes(max_chi);
+  const int M2 = max_chi * max_chi;
+  cd *Af = reinterpret_cast<cd *>(base);
+  cd *Vf = Af + M2, *Ab = Vf + M2, *Vb = Ab + M2, *Qf = Vb + M2, *Qb = Qf + M2, *C = Qb + M2, *W = C + M2;
+  double *wf = reinterpret_cast<double *>(W + M2);
+  double *wb = wf + max_chi, *sv = wb + max_chi;
+  int *perm = reinterpret_cast<int *>(sv + max_chi);
+  const int tid = threadIdx.x, nt = blockDim.x;
+
+  for (int e = blockIdx.x; e < g.n_edges; e += gridDim.x) {
+    const int h0 = g.edge_half[2 * e], h1 = g.edge_half[2 * e + 1];
+    const int c = g.edge_chi[e];
+    const cd *mf = n2e + g.half_msg_off[h0];
+    const cd *mb = n2e + g.half_msg_off[h1];
+    for (int i = tid; i < c * c; i += nt) {
+      Af[i] = mf[i];
+      Ab[i] = mb[i];
+    }
+    __syncthreads();
+    herm_eigh(Af, c, Vf, c, c, wf, rots, red);
+    herm_eigh(Ab, c, Vb, c, c, wb, rots, red);
+    // Af <- sqrt(m_f), Qf <- sqrt(m_f)^+ (safe), same for b.
+    for (int idx = tid; idx < c * c; idx += nt) {
+      const int i = idx / c, j = idx % c;
+      cd sf = czero(), sif = czero(), sb = czero(), sib = czero();
+      for (int k = 0; k < c; ++k) {
+        cd pf = cmul(Vf[i * c + k], cconj(Vf[j * c + k]));
+        cd pb = cmul(Vb[i * c + k], cconj(Vb[j * c + k]));
+        sf = cadd(sf, cscale(pf, sqrt(safe_truncate(wf[k], eps))));
+        sif = cadd(sif, cscale(pf, sqrt(safe_inverse(wf[k], eps))));
+        sb = cadd(sb, cscale(pb, sqrt(safe_truncate(wb[k], eps))));
+        sib = cadd(sib, cscale(pb, sqrt(safe_inverse(wb[k], eps))));
+      }
+      Af[idx] = sf;
+      Qf[idx] = sif;
+      Ab[idx] = sb;
+      Qb[idx] = sib;
+    }
+    __syncthreads();
+    // C = sqrt(m_f) sqrt(m_b)^T, column-major for the one-sided Jacobi.
+    for (int idx = tid; idx < c * c; idx += nt) {
+      const int i = idx / c, j = idx % c;
+      cd acc = czero();
+      for (int k = 0; k < c; ++k) cfma(acc, Af[i * c + k], Ab[j * c + k]);
+      C[j * c + i] = acc;
+    }
+    __syncthreads();
+    hestenes(C, c, c, c, W, c, sv, flag, red);
+    sort_desc(sv, c, perm);
+    // lambda = sigma / |sigma|, truncated; U (into Af) and V^* (into Ab)
+    // masked and Frobenius-normalised.
+    double nrm2 = 0.0;
+    for (int j = tid; j < c; j += nt) nrm2 += sv[j] * sv[j];
+    nrm2 = block_sum(nrm2, red);
+    const double inv_n = 1.0 / sqrt(nrm2);
+    double *lam = lambdas + g.edge_lam_off[e];
+    for (int j = tid; j < c; j += nt) lam[j] = safe_truncate(sv[perm[j]] * inv_n, eps);
+    __syncthreads();
+    double un = 0.0, vn = 0.0;
+    for (int idx = tid; idx < c * c; idx += nt) {
+      const int i = idx / c, j = idx % c;  // row i, column j
+      const int pj = perm[j];
+      const bool keep = lam[j] > eps && sv[pj] > 0.0;
+      cd u = keep ? cscale(C[pj * c + i], 1.0 / sv[pj]) : czero();
+      cd w = keep ? cconj(W[pj * c + i]) : czero();
+      Af[i * c + j] = u;
+      Ab[i * c + j] = w;
+      un += cabs2(u);
+      vn += cabs2(w);
+    }
+    un = block_sum(un, red);
+    vn = block_sum(vn, red);
+    const double iu = 1.0 / sqrt(un), iv = 1.0 / sqrt(vn);
+    cd *Gf = orth + g.half_msg_off[h0];
+    cd *Gb = orth + g.half_msg_off[h1];
+    for (int idx = tid; idx < c * c; idx += nt) {
+      const int i = idx / c, j = idx % c;
+      cd af = czero(), ab = czero();
+      for (int k = 0; k < c; ++k) {
+        cfma(af, Qf[i * c + k], Af[k * c + j]);
+        cfma(ab, Qb[i * c + k], Ab[k * c + j]);
+      }
+      Gf[idx] = cscale(af, iu);
+      Gb[idx] = cscale(ab, iv);
+    }
+    __syncthreads();
+  }
+}
+
+// ----------------------------------------------------------------- absorb
+__global__ void __launch_bounds__(GAUGE_THREADS) absorb_kernel(dqz_graph_t g, const cd *__restrict__ Tin,
+                                                                const cd *__restrict__ orth, cd *Tout, int max_size,
+                                                                cd *scratch) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double *red = reinterpret_cast<double *>(smem_raw);
+  cd *bufA = scratch ? scratch + (long long)blockIdx.x * 2 * max_size
+                     : reinterpret_cast<cd *>(smem_raw + 48 * sizeof(double));
+  cd *bufB = bufA + max_size;
+  for (int v = blockIdx.x; v < g.n_nodes; v += gridDim.x) {
+    NodeShape s;
+    load_shape(g, v, s);
+    const cd *T = Tin + g.node_off[v];
+    for (long long i = threadIdx.x; i < s.size; i += blockDim.x) bufA[i] = T[i];
+    __syncthreads();
+    cd *cur = bufA, *nxt = bufB;
+    long long L = 1;
+    for (int f = 0; f < s.k; ++f) {
+      const int q = s.dims[f];
+      const long long R = s.size / L / q;
+      const cd *G = orth + g.half_msg_off[s.half0 + f];
+      // new[.., j, ..] = sum_a G[a][j] T[.., a, ..]
+      mode_product<false>(cur, nxt, L, q, q, R, G, 1, q);
+      __syncthreads();
+      cd *t = cur;
+      cur = nxt;
+      nxt = t;
+      L *= q;
+    }
+    double n2 = 0.0;
+    for (long long i = threadIdx.x; i < s.size; i += blockDim.x) n2 += cabs2(cur[i]);
+    n2 = block_sum(n2, red);
+    const double inv = 1.0 / sqrt(n2);
+    cd *O = Tout + g.node_off[v];
+    for (long long i = threadIdx.x; i < s.size; i += blockDim.x) O[i] = cscale(cur[i], inv);
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------- vidal distance
+// partial[h] = trace norm of (R/tr R - ideal) for bond e of node v (h = (v,e)).
+__global__ void __launch_bounds__(GAUGE_THREADS) vidal_distance_kernel(dqz_graph_t g, const cd *__restrict__ Tall,
+                                                                        const double *__restrict__ lambdas,
+                                                                        double eps, double *partial, int max_chi) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double *red = reinterpret_cast<double *>(smem_raw);
+  Rot *rots = reinterpret_cast<Rot *>(smem_raw + 48 * sizeof(double));
+  cd *Rm = reinterpret_cast<cd *>(rots + (DQZ_MAX_CHI / 2 + 1));
+  cd *Vm = Rm + max_chi * max_chi;
+  double *w = reinterpret_cast<double *>(Vm + max_chi * max_chi);
+  __shared__ cd trace_sh;
+  __shared__ int count_sh;
+  const int nh = g.n_halves;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int h = blockIdx.x; h < nh; h += gridDim.x) {
+    const int v = g.half_node[h];
+    NodeShape s;
+    load_shape(g, v, s);
+    const int e = h - s.half0;
+    const int ce = s.dims[e];
+    const cd *T = Tall + g.node_off[v];
+    const long long Re = s.stride[e];
+    const long long P = s.size / ce;
+    const double *lam[DQZ_MAX_DEGREE];
+    for (int f = 0; f < s.k; ++f) lam[f] = lambdas + g.edge_lam_off[g.half_edge[s.half0 + f]];
+    const int npair = ce * (ce + 1) / 2;
+    for (int pi = warp; pi < npair; pi += nw) {
+      // pair index -> (ap <= a)
+      int ap = 0, rem = pi;
+      while (rem >= ce - ap) {
+        rem -= ce - ap;
+        ++ap;
+      }
+      const int a = ap + rem;
+      cd acc = czero();
+      for (long long x = lane; x < P; x += 32) {
+        const long long l = x / Re, r = x - l * Re;
+        const long long o0 = (l * ce) * Re + r;  // offset with a_e = 0
+        double wt = 1.0;
+        for (int f = 0; f < s.k; ++f) {
+          if (f == e) continue;
+          const int idx = (int)((o0 / s.stride[f]) % s.dims[f]);
+          const double lv = lam[f][idx];
+          wt *= lv * lv;
+        }
+        cfmac(acc, T[o0 + ap * Re], cscale(T[o0 + a * Re], wt));
+      }
+      acc = warp_csum(acc);
+      if (lane == 0) {
+        Rm[ap * ce + a] = acc;
+        Rm[a * ce + ap] = cconj(acc);
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      cd tr = czero();
+      for (int i = 0; i < ce; ++i) tr = cadd(tr, Rm[i * ce + i]);
+      trace_sh = tr;
+    }
+    __syncthreads();
+    const cd tr = trace_sh;
+    for (int i = threadIdx.x; i < ce * ce; i += blockDim.x) Rm[i] = cdiv(Rm[i], tr);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int cnt = 0;
+      for (int i = 0; i < ce; ++i) cnt += Rm[i * ce + i].x > eps ? 1 : 0;
+      count_sh = cnt;
+    }
+    __syncthreads();
+    const double idv = 1.0 / (double)count_sh;
+    for (int i = threadIdx.x; i < ce; i += blockDim.x)
+      if (Rm[i * ce + i].x > eps) Rm[i * ce + i].x -= idv;
+    __syncthreads();
+    herm_eigh(Rm, ce, Vm, ce, ce, w, rots, red);
+    double t = 0.0;
+    for (int i = threadIdx.x; i < ce; i += blockDim.x) t += fabs(w[i]);
+    t = block_sum(t, red);
+    if (threadIdx.x == 0) partial[h] = t;
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------- symmetric gauge
+__global__ void __launch_bounds__(GAUGE_THREADS) symmetric_kernel(dqz_graph_t g, const cd *__restrict__ Tin,
+                                                                   const double *__restrict__ lambdas, double eps,
+                                                                   cd *Tout) {
+  __shared__ double red[48];
+  for (int v = blockIdx.x; v < g.n_nodes; v += gridDim.x) {
+    NodeShape s;
+    load_shape(g, v, s);
+    const double *lam[DQZ_MAX_DEGREE];
+    for (int f = 0; f < s.k; ++f) lam[f] = lambdas + g.edge_lam_off[g.half_edge[s.half0 + f]];
+    const cd *T = Tin + g.node_off[v];
+    cd *O = Tout + g.node_off[v];
+    double n2 = 0.0;
+    for (long long i = threadIdx.x; i < s.size; i += blockDim.x) {
+      double wt = 1.0;
+      for (int f = 0; f < s.k; ++f) wt *= sqrt(safe_truncate(lam[f][(i / s.stride[f]) % s.dims[f]], eps));
+      n2 += cabs2(T[i]) * wt * wt;
+    }
+    n2 = block_sum(n2, red);
+    const double inv = 1.0 / sqrt(n2);
+    for (long long i = threadIdx.x; i < s.size; i += blockDim.x) {
+      double wt = 1.0;
+      for (int f = 0; f < s.k; ++f) wt *= sqrt(safe_truncate(lam[f][(i / s.stride[f]) % s.dims[f]], eps));
+      O[i] = cscale(T[i], wt * inv);
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void lambdas_to_messages_kernel(dqz_graph_t g, const double *__restrict__ lambdas, cd *n2e, cd *e2n) {
+  const int nh = g.n_halves;
+  const int wpb = blockDim.x >> 5, lane = threadIdx.x & 31;
+  for (int h = blockIdx.x * wpb + (threadIdx.x >> 5); h < nh; h += gridDim.x * wpb) {
+    const int e = g.half_edge[h];
+    if (e < 0) continue;
+    const int c = g.edge_chi[e];
+    const double *lam = lambdas + g.edge_lam_off[e];
+    cd *a = n2e + g.half_msg_off[h];
+    cd *b = e2n + g.half_msg_off[h];
+    for (int i = lane; i < c * c; i += 32) {
+      cd val = (i / c == i % c) ? mk(lam[i / c], 0.0) : czero();
+      a[i] = val;
+      b[i] = val;
+    }
+  }
+}
+
+// -------------------------------------------------------- density matrices
+__global__ void __launch_bounds__(GAUGE_THREADS) density_kernel(dqz_graph_t g, const cd *__restrict__ Tall,
+                                                                 const cd *__restrict__ e2n,
+                                                                 const int32_t *__restrict__ nodes, int n_nodes,
+                                                                 cd *rho, int max_size, cd *scratch) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cd *bufA = scratch ? scratch + (long long)blockIdx.x * 2 * max_size : reinterpret_cast<cd *>(smem_raw);
+  cd *bufB = bufA + max_size;
+  __shared__ cd rho_sh[DQZ_MAX_PHYS * DQZ_MAX_PHYS];
+  __shared__ cd trace_sh;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int item = blockIdx.x; item < n_nodes; item += gridDim.x) {
+    const int v = nodes[item];
+    NodeShape s;
+    load_shape(g, v, s);
+    const cd *T = Tall + g.node_off[v];
+    for (long long i = threadIdx.x; i < s.size; i += blockDim.x) bufA[i] = T[i];
+    __syncthreads();
+    cd *cur = bufA, *nxt = bufB;
+    long long L = 1;
+    for (int f = 0; f < s.k; ++f) {
+      const int q = s.dims[f];
+      const long long R = s.size / L / q;
+      const cd *m = e2n + g.half_msg_off[s.half0 + f];
+      mode_product<false>(cur, nxt, L, q, q, R, m, q, 1);
+      __syncthreads();
+      cd *t = cur;
+      cur = nxt;
+      nxt = t;
+      L *= q;
+    }
+    const int d = s.d;
+    const long long B = s.size / d;
+    for (int p = warp; p < d * d; p += nw) {
+      const int si = p / d, sj = p % d;
+      cd acc = czero();
+      for (long long b = lane; b < B; b += 32) cfmac(acc, T[b * d + sj], cur[b * d + si]);
+      acc = warp_csum(acc);
+      if (lane == 0) rho_sh[si * d + sj] = acc;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      cd tr = czero();
+      for (int i = 0; i < d; ++i) tr = cadd(tr, rho_sh[i * d + i]);
+      trace_sh = tr;
+    }
+    __syncthreads();
+    cd *out = rho + (long long)item * DQZ_MAX_PHYS * DQZ_MAX_PHYS;
+    for (int i = threadIdx.x; i < d * d; i += blockDim.x) out[i] = cdiv(rho_sh[i], trace_sh);
+    __syncthreads();
+  }
+}
+
+size_t eigh_smem(int max_chi) {
+  return 48 * sizeof(double) + (DQZ_MAX_CHI / 2 + 1) * sizeof(Rot) + 4 * sizeof(int);
+}
+
+}  // namespace
+
+extern "C" size_t dqz_vidal_edges_scratch_bytes(int32_t n_edges, int32_t max_chi) {
+  size_t need = eigh_smem(max_chi) + vidal_edge_bytes(max_chi);
+  if (need <= SMEM_LIMIT) return 0;
+  int grid = n_edges < SCRATCH_GRID ? n_edges : SCRATCH_GRID;
+  return (size_t)grid * vidal_edge_bytes(max_chi);
+}
+
+extern "C" int dqz_vidal_edges(const dqz_graph_t *g, const void *n2e, double eps, void *orth, double *lambdas,
+                               int32_t max_chi, void *scratch, cudaStream_t stream) {
+  if (!g || !n2e || !orth || !lambdas) return DQZ_ERR_ARG;
+  if (max_chi <= 0 || max_chi > DQZ_MAX_CHI) return DQZ_ERR_UNSUPPORTED;
+  if (g->n_edges == 0) return DQZ_OK;
+  size_t need = eigh_smem(max_chi) + vidal_edge_bytes(max_chi);
+  const bool use_scratch = need > SMEM_LIMIT;
+  if (use_scratch && !scratch) return DQZ_ERR_ARG;
+  size_t smem = use_scratch ? eigh_smem(max_chi) : need;
+  cudaFuncSetAttribute(vidal_edges_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_LIMIT);
+  int grid = use_scratch ? (g->n_edges < SCRATCH_GRID ? g->n_edges : SCRATCH_GRID) : g->n_edges;
+  vidal_edges_kernel<<<grid, GAUGE_THREADS, smem, stream>>>(*g, (const cd *)n2e, eps, (cd *)orth, lambdas, max_chi,
+                                                           use_scratch ? (unsigned char *)scratch : nullptr);
+  DQZ_CHECK_LAUNCH();
+  return DQZ_OK;
+}
+
+extern "C" size_t dqz_absorb_scratch_bytes(int32_t n_nodes, int32_t max_size) {
+  size_t need = 48 * sizeof(double) + 2 * (size_t)max_size * sizeof(cd);
+  if (need <= SMEM_LIMIT) return 0;
+  int grid = n_nodes < SCRATCH_GRID ? n_nodes : SCRATCH_GRID;
+  return (size_t)grid * 2 * (size_t)max_size * sizeof(cd);
+}
+
+extern "C" int dqz_absorb(const dqz_graph_t *g, const void *tensors_in, const void *orth, void *tensors_out,
+                          int32_t max_size, void *scratch, cudaStream_t stream) {
+  if (!g || !tensors_in || !orth || !tensors_out || max_size <= 0) return DQZ_ERR_ARG;
+  if (g->n_nodes == 0) return DQZ_OK;
+  size_t need = 48 * sizeof(double) + 2 * (size_t)max_size * sizeof(cd);
+  const bool use_scratch = need > SMEM_LIMIT;
+  if (use_scratch && !scratch) return DQZ_ERR_ARG;
+  cudaFuncSetAttribute(absorb_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_LIMIT);
+  int grid = use_scratch ? (g->n_nodes < SCRATCH_GRID ? g->n_nodes : SCRATCH_GRID) : g->n_nodes;
+  absorb_kernel<<<grid, GAUGE_THREADS, use_scratch ? 48 * sizeof(double) : need, stream>>>(
+      *g, (const cd *)tensors_in, (const cd *)orth, (cd *)tensors_out, max_size,
+      use_scratch ? (cd *)scratch : nullptr);
+  DQZ_CHECK_LAUNCH();
+  return DQZ_OK;
+}
+
+extern "C" int dqz_vidal_distance(const dqz_graph_t *g, const void *tensors, const double *lambdas, double eps,
+                                  double *partial, double *out, int32_t max_chi, cudaStream_t stream) {
+  if (!g || !tensors || !lambdas || !partial || !out) return DQZ_ERR_ARG;
+  if (max_chi <= 0 || max_chi > DQZ_MAX_CHI) return DQZ_ERR_UNSUPPORTED;
+  const int nh = g->n_halves;
+  if (nh == 0 || g->n_edges == 0) return DQZ_ERR_ARG;
+  size_t smem = eigh_smem(max_chi) + 2 * (size_t)max_chi * max_chi * sizeof(cd) + (size_t)max_chi * sizeof(double);
+  cudaFuncSetAttribute(vidal_distance_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_LIMIT);
+  vidal_distance_kernel<<<nh, GAUGE_THREADS, smem, stream>>>(*g, (const cd *)tensors, lambdas, eps, partial,
+                                                             max_chi);
+  DQZ_CHECK_LAUNCH();
+  return dqz_reduce_sum(partial, nh, 1.0 / (2.0 * g->n_edges), out, stream);
+}
+
+extern "C" int dqz_symmetric_gauge(const dqz_graph_t *g, const void *tensors_in, const double *lambdas, double eps,
+                                   void *tensors_out, cudaStream_t stream) {
+  if (!g || !tensors_in || !lambdas || !tensors_out) return DQZ_ERR_ARG;
+  if (g->n_nodes == 0) return DQZ_OK;
+  symmetric_kernel<<<g->n_nodes, GAUGE_THREADS, 0, stream>>>(*g, (const cd *)tensors_in, lambdas, eps,
+                                                              (cd *)tensors_out);
+  DQZ_CHECK_LAUNCH();
+  return DQZ_OK;
+}
+
+extern "C" int dqz_lambdas_to_messages(const dqz_graph_t *g, const double *lambdas, void *n2e, void *e2n,
+                                       int32_t max_chi, cudaStream_t stream) {
+  if (!g || !lambdas || !n2e || !e2n) return DQZ_ERR_ARG;
+  if (max_chi <= 0 || max_chi > DQZ_MAX_CHI) return DQZ_ERR_UNSUPPORTED;
+  const int nh = g->n_halves;
+  if (nh == 0) return DQZ_OK;
+  lambdas_to_messages_kernel<<<(nh + 7) / 8, 256, 0, stream>>>(*g, lambdas, (cd *)n2e, (cd *)e2n);
+  DQZ_CHECK_LAUNCH();
+  return DQZ_OK;
+}
+
+extern "C" size_t dqz_density_scratch_bytes(int32_t n_nodes, int32_t max_size) {
+  size_t need = 2 * (size_t)max_size * sizeof(cd);
+  if (need <= SMEM_LIMIT) return 0;
+  int grid = n_nodes < SCRATCH_GRID ? n_nodes : SCRATCH_GRID;
+  return (size_t)grid * 2 * (size_t)max_size * sizeof(cd);
+}
+
+extern "C" int dqz_density_matrices(const dqz_graph_t *g, const void *tensors, const void *e2n,
+                                    const int32_t *nodes, int32_t n_nodes, void *rho, int32_t max_size,
+                                    void *scratch, cudaStream_t stream) {
+  if (!g || !tensors || !e2n || !nodes || !rho || n_nodes < 0 || max_size <= 0) return DQZ_ERR_ARG;
+  if (n_nodes == 0) return DQZ_OK;
+  size_t need = 2 * (size_t)max_size * sizeof(cd);
+  const bool use_scratch = need > SMEM_LIMIT;
+  if (use_scratch && !scratch) return DQZ_ERR_ARG;
+  cudaFuncSetAttribute(density_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_LIMIT);
+  int grid = use_scratch ? (n_nodes < SCRATCH_GRID ? n_nodes : SCRATCH_GRID) : n_nodes;
+  density_kernel<<<grid, GAUGE_THREADS, use_scratch ? 0 : need, stream>>>(
+      *g, (const cd *)tensors, (const cd *)e2n, nodes, n_nodes, (cd *)rho, max_size,
+      use_scratch ? (cd *)scratch : nullptr);
+  DQZ_CHECK_LAUNCH();
+  return DQZ_OK;
+}

@@ -1,0 +1,320 @@
+// CTA-cooperative small dense linear algebra in FP64 for libdqz:
+//  * herm_eigh  -- parallel cyclic Jacobi for Hermitian n x n (n <= 128), the
+//                  message eigendecompositions of tensor_ops.py:115-120 and the
+//                  trace norm of tensor_ops.py:173 (Hermitian operand).
+//  * hestenes   -- one-sided Jacobi SVD on the columns of an m x n matrix, the
+//                  SVDs of tensor_ops.py:121 and :360.
+//  * householder_qr / apply_q -- LAPACK-convention (zgeqr2 / zung2r) QR, the
+//                  QR of tensor_ops.py:288.
+// Pairs are scheduled with the round-robin (circle) ordering, so each step
+// rotates n/2 disjoint index pairs at once.
+#pragma once
+
+#include "common.cuh"
+
+namespace dqz {
+
+struct Rot {
+  int p, q;
+  cd j00, j01, j10, j11;
+};
+
+// Pair i of round-robin step `step` for an even count np: (0, step+1) for
+// i == 0, otherwise (step+i, step-i) modulo np-1, shifted by one.
+__device__ __forceinline__ void rr_pair(int step, int i, int np, int &p, int &q) {
+  const int m = np - 1;
+  if (i == 0) {
+    p = 0;
+    q = step % m + 1;
+  } else {
+    p = (step + i) % m + 1;
+    q = ((step - i) % m + m) % m + 1;
+  }
+  if (p > q) {
+    int t = p;
+    p = q;
+    q = t;
+  }
+}
+
+// Unitary J = D R that diagonalises the Hermitian 2x2 [[a, c], [conj(c), b]]
+// (a, b real): D = diag(c/|c|, 1), R the real Jacobi rotation of
+// [[a, |c|], [|c|, b]]. Returns false when c is negligible.
+__device__ __forceinline__ bool jacobi_rot(double a, double b, cd c, Rot &r) {
+  double ac = sqrt(cabs2(c));
+  if (!(ac > 0.0) || ac < 1e-300) return false;
+  double tau = (b - a) / (2.0 * ac);
+  double t = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
+  double cs = 1.0 / sqrt(1.0 + t * t);
+  double sn = t * cs;
+  cd ph = mk(c.x / ac, c.y / ac);
+  r.j00 = cscale(ph, cs);
+  r.j01 = cscale(ph, sn);
+  r.j10 = mk(-sn, 0.0);
+  r.j11 = mk(cs, 0.0);
+  return true;
+}
+
+// Hermitian eigendecomposition. A (n x n, row-major, lda) is destroyed; on
+// return w[i] holds eigenvalue i and column i of V (row-major, ldv) the
+// matching eigenvector (unsorted). rots: >= n/2+1 entries, red: 33 doubles,
+// all in shared memory.
+static __device__ void herm_eigh(cd *A, int lda, cd *V, int ldv, int n, double *w, Rot *rots, double *red,
+                          int max_sweeps = 40) {
+  const int tid = threadIdx.x, nt = blockDim.x;
+  for (int i = tid; i < n * n; i += nt) V[(i / n) * ldv + (i % n)] = (i / n == i % n) ? mk(1.0, 0.0) : czero();
+  __syncthreads();
+  const int np = n + (n & 1);
+  const int npairs = np / 2;
+  if (n > 1) {
+    for (int sweep = 0; sweep < max_sweeps; ++sweep) {
+      double off = 0.0, dia = 0.0;
+      for (int i = tid; i < n * n; i += nt) {
+        int r = i / n, c = i % n;
+        double v = cabs2(A[r * lda + c]);
+        if (r == c)
+          dia += v;
+        else
+          off += v;
+      }
+      off = block_sum(off, red);
+      dia = block_sum(dia, red);
+      if (off == 0.0 || off <= 1e-30 * dia) break;
+      for (int step = 0; step < np - 1; ++step) {
+        for (int i = tid; i < npairs; i += nt) {
+          int p, q;
+          rr_pair(step, i, np, p, q);
+          Rot r;
+          r.p = -1;
+          r.q = q;
+          if (q < n) {
+            double a = A[p * lda + p].x, b = A[q * lda + q].x;
+            cd c = A[p * lda + q];
+            double ac2 = cabs2(c);
+            if (ac2 > 0.0 && ac2 >= 1e-36 * (a * a + b * b) && jacobi_rot(a, b, c, r)) r.p = p;
+          }
+          rots[i] = r;
+        }
+        __syncthreads();
+        // A <- A J and V <- V J on columns (p, q)
+        for (int idx = tid; idx < npairs * n; idx += nt) {
+          const Rot &r = rots[idx / n];
+          if (r.p < 0) continue;
+          int row = idx % n;
+          cd x = A[row * lda + r.p], y = A[row * lda + r.q];
+          A[row * lda + r.p] = cadd(cmul(x, r.j00), cmul(y, r.j10));
+          A[row * lda + r.q] = cadd(cmul(x, r.j01), cmul(y, r.j11));
+          x = V[row * ldv + r.p];
+          y = V[row * ldv + r.q];
+          V[row * ldv + r.p] = cadd(cmul(x, r.j00), cmul(y, r.j10));
+          V[row * ldv + r.q] = cadd(cmul(x, r.j01), cmul(y, r.j11));
+        }
+        __syncthreads();
+        // A <- J^H A on rows (p, q)
+        for (int idx = tid; idx < npairs * n; idx += nt) {
+          const Rot &r = rots[idx / n];
+          if (r.p < 0) continue;
+          int col = idx % n;
+          cd x = A[r.p * lda + col], y = A[r.q * lda + col];
+          A[r.p * lda + col] = cadd(cmulc(r.j00, x), cmulc(r.j10, y));
+          A[r.q * lda + col] = cadd(cmulc(r.j01, x), cmulc(r.j11, y));
+        }
+        __syncthreads();
+      }
+    }
+  }
+  for (int i = tid; i < n; i += nt) w[i] = A[i * lda + i].x;
+  __syncthreads();
+}
+
+// One-sided Jacobi SVD on the columns of A (m x n, column-major, lda), m >= n
+// is not required but only min(m, n) columns come out non-zero when m < n.
+// On return column j of A is s_j u_j, V (n x n, column-major, ldv) holds the
+// right singular vectors, s[j] = |A_j| (unsorted). One warp rotates a pair.
+static __device__ void hestenes(cd *A, int lda, int m, int n, cd *V, int ldv, double *s, int *flag, double *red,
+                         int max_sweeps = 60) {
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const int lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
+  for (int i = tid; i < n * n; i += nt) V[(i / n) * ldv + (i % n)] = (i / n == i % n) ? mk(1.0, 0.0) : czero();
+  const double tol = 1.1e-16 * sqrt((double)(m > 1 ? m : 1)) * 2.0;
+  const int np = n + (n & 1);
+  const int npairs = np / 2;
+  __syncthreads();
+  if (n > 1) {
+    for (int sweep = 0; sweep < max_sweeps; ++sweep) {
+      if (tid == 0) *flag = 0;
+      __syncthreads();
+      for (int step = 0; step < np - 1; ++step) {
+        for (int i = warp; i < npairs; i += nw) {
+          int p, q;
+          rr_pair(step, i, np, p, q);
+          if (q >= n) continue;
+          cd *ap = A + (long long)p * lda, *aq = A + (long long)q * lda;
+          double al = 0.0, be = 0.0;
+          cd ga = czero();
+          for (int r = lane; r < m; r += 32) {
+            cd x = ap[r], y = aq[r];
+            al += cabs2(x);
+            be += cabs2(y);
+            cfmac(ga, x, y);
+          }
+          al = warp_sum(al);
+          be = warp_sum(be);
+          ga = warp_csum(ga);
+          double ag = sqrt(cabs2(ga));
+          if (!(al > 0.0) || !(be > 0.0) || !(ag > tol * sqrt(al) * sqrt(be))) continue;
+          Rot r;
+          if (!jacobi_rot(al, be, ga, r)) continue;
+          if (lane == 0) *flag = 1;
+          for (int k = lane; k < m; k += 32) {
+            cd x = ap[k], y = aq[k];
+            ap[k] = cadd(cmul(x, r.j00), cmul(y, r.j10));
+            aq[k] = cadd(cmul(x, r.j01), cmul(y, r.j11));
+          }
+          cd *vp = V + (long long)p * ldv, *vq = V + (long long)q * ldv;
+          for (int k = lane; k < n; k += 32) {
+            cd x = vp[k], y = vq[k];
+            vp[k] = cadd(cmul(x, r.j00), cmul(y, r.j10));
+            vq[k] = cadd(cmul(x, r.j01), cmul(y, r.j11));
+          }
+        }
+        __syncthreads();
+      }
+      if (*flag == 0) break;
+      __syncthreads();
+    }
+  }
+  for (int j = warp; j < n; j += nw) {
+    double t = 0.0;
+    for (int r = lane; r < m; r += 32) t += cabs2(A[(long long)j * lda + r]);
+    t = warp_sum(t);
+    if (lane == 0) s[j] = sqrt(t);
+  }
+  __syncthreads();
+}
+
+// perm[j] = index of the j-th largest s (stable). n <= blockDim.
+static __device__ void sort_desc(const double *s, int n, int *perm) {
+  for (int j = threadIdx.x; j < n; j += blockDim.x) {
+    int rank = 0;
+    double sj = s[j];
+    for (int i = 0; i < n; ++i) {
+      double si = s[i];
+      if (si > sj || (si == sj && i < j)) ++rank;
+    }
+    perm[rank] = j;
+  }
+  __syncthreads();
+}
+
+// Completes the columns of U (m x ncol, column-major, ldu) flagged in
+// `null_col` to an orthonormal set: each flagged column becomes the first unit
+// vector e_c, orthogonalised (twice) against all accepted columns, that keeps
+// norm > 0.5. Run by warp 0; `acc` must hold the non-null flags on entry.
+static __device__ void complete_orthonormal(cd *U, int ldu, int m, int ncol, int *acc) {
+  const int lane = threadIdx.x & 31;
+  if ((threadIdx.x >> 5) == 0) {
+    int cand = 0;
+    for (int j = 0; j < ncol; ++j) {
+      if (acc[j]) continue;
+      cd *uj = U + (long long)j * ldu;
+      bool done = false;
+      while (!done && cand < m) {
+        for (int r = lane; r < m; r += 32) uj[r] = (r == cand) ? mk(1.0, 0.0) : czero();
+        __syncwarp();
+        for (int pass = 0; pass < 2; ++pass) {
+          for (int i = 0; i < ncol; ++i) {
+            if (!acc[i]) continue;
+            const cd *ui = U + (long long)i * ldu;
+            cd dot = czero();
+            for (int r = lane; r < m; r += 32) cfmac(dot, ui[r], uj[r]);
+            dot = warp_csum(dot);
+            for (int r = lane; r < m; r += 32) uj[r] = csub(uj[r], cmul(ui[r], dot));
+            __syncwarp();
+          }
+        }
+        double nn = 0.0;
+        for (int r = lane; r < m; r += 32) nn += cabs2(uj[r]);
+        nn = warp_sum(nn);
+        ++cand;
+        if (nn > 0.25) {
+          double inv = 1.0 / sqrt(nn);
+          for (int r = lane; r < m; r += 32) uj[r] = cscale(uj[r], inv);
+          __syncwarp();
+          if (lane == 0) acc[j] = 1;
+          __syncwarp();
+          done = true;
+        }
+      }
+    }
+  }
+  __syncthreads();
+}
+
+// LAPACK-convention Householder QR of A (M x K, column-major, ld = M):
+// H_j = I - tau_j v_j v_j^H, v_j[j] = 1, v_j below the diagonal of column j,
+// R on and above the diagonal, beta real (zlarfg). H_j^H is applied to the
+// trailing columns (zgeqr2).
+static __device__ void householder_qr(cd *A, int M, int K, cd *tau, double *red) {
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const int lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
+  const int kk = M < K ? M : K;
+  for (int j = 0; j < kk; ++j) {
+    cd *col = A + (long long)j * M;
+    double s = 0.0;
+    for (int r = j + 1 + tid; r < M; r += nt) s += cabs2(col[r]);
+    s = block_sum(s, red);
+    cd alpha = col[j];
+    cd t;
+    if (s == 0.0 && alpha.y == 0.0) {
+      t = czero();
+    } else {
+      double beta = -copysign(sqrt(cabs2(alpha) + s), alpha.x);
+      t = mk((beta - alpha.x) / beta, -alpha.y / beta);
+      cd sc = cdiv(mk(1.0, 0.0), mk(alpha.x - beta, alpha.y));
+      for (int r = j + 1 + tid; r < M; r += nt) col[r] = cmul(col[r], sc);
+      __syncthreads();
+      if (tid == 0) col[j] = mk(beta, 0.0);
+    }
+    if (tid == 0) tau[j] = t;
+    __syncthreads();
+    if (t.x != 0.0 || t.y != 0.0) {
+      for (int c = j + 1 + warp; c < K; c += nw) {
+        cd *ac = A + (long long)c * M;
+        cd w = czero();
+        if (lane == 0) w = ac[j];
+        for (int r = j + 1 + lane; r < M; r += 32) cfmac(w, col[r], ac[r]);
+        w = warp_csum(w);
+        cd f = cmulc(t, w);  // conj(tau) * w
+        if (lane == 0) ac[j] = csub(ac[j], f);
+        for (int r = j + 1 + lane; r < M; r += 32) ac[r] = csub(ac[r], cmul(col[r], f));
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// X <- Q X with Q = H_0 ... H_{kk-1} from householder_qr; X is M x p,
+// column-major (ldx).
+static __device__ void apply_q(const cd *A, int M, int kk, const cd *tau, cd *X, int ldx, int p) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int j = kk - 1; j >= 0; --j) {
+    cd t = tau[j];
+    if (t.x != 0.0 || t.y != 0.0) {
+      const cd *v = A + (long long)j * M;
+      for (int c = warp; c < p; c += nw) {
+        cd *xc = X + (long long)c * ldx;
+        cd w = czero();
+        if (lane == 0) w = xc[j];
+        for (int r = j + 1 + lane; r < M; r += 32) cfmac(w, v[r], xc[r]);
+        w = warp_csum(w);
+        cd f = cmul(t, w);
+        if (lane == 0) xc[j] = csub(xc[j], f);
+        for (int r = j + 1 + lane; r < M; r += 32) xc[r] = csub(xc[r], cmul(v[r], f));
+      }
+    }
+    __syncthreads();
+  }
+}
+
+}  // namespace dqz

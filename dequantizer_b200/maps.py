@@ -1,0 +1,328 @@
+"""Graph-wide maps with the reference's dict-in / dict-out interface, run on
+the GPU through libdqz.
+
+Each factory mirrors its reference counterpart and returns a pure callable
+over ``Dict[NodeID, Tensor]`` / ``Dict[MessageID, Tensor]`` /
+``Dict[EdgeID, Tensor]`` that returns NEW dicts (values are views into fresh
+device arenas; inputs are never modified):
+
+* get_belief_propagation_map     -- mappings/belief_propagation.py:24-64
+* get_vidal_gauge_fixing_map     -- mappings/vidal_gauge.py:21-63
+* get_vidal_gauge_distance_map   -- mappings/vidal_distance.py:17-42
+* get_symmetric_gauge_fixing_map -- mappings/symmetric_gauge.py:17-39
+* lambdas2messages               -- mappings/symmetric_gauge.py:50-61
+* messages_frob_distance         -- mappings/messages_distance.py:14-22
+* get_one_side_density_matrix    -- mappings/density_matrix.py:16-37
+
+Tensors must be complex128 CUDA tensors (anything else is converted on the
+device; host arrays are copied to the device first).
+"""
+
+from typing import Dict, List
+
+import numpy as np
+import torch
+
+from . import _lib
+from .graph import Edge, MessageID, Node
+from .layout import GraphLayout, layout_from_traverser
+
+
+def as_device(x) -> torch.Tensor:
+    """complex128 CUDA tensor from a tensor or array (host data is copied)."""
+    if isinstance(x, torch.Tensor):
+        t = x
+    else:
+        t = torch.from_numpy(np.asarray(x))
+    if not t.is_cuda:
+        if not torch.cuda.is_available():
+            raise RuntimeError("dequantizer_b200 runs on the GPU only and no CUDA device is available")
+        t = t.to(_lib.device())
+    if t.dtype != torch.complex128:
+        t = t.to(torch.complex128)
+    return t.contiguous()
+
+
+def as_device_real(x) -> torch.Tensor:
+    t = x if isinstance(x, torch.Tensor) else torch.from_numpy(np.asarray(x))
+    if not t.is_cuda:
+        if not torch.cuda.is_available():
+            raise RuntimeError("dequantizer_b200 runs on the GPU only and no CUDA device is available")
+        t = t.to(_lib.device())
+    if t.is_complex():
+        t = t.real
+    return t.to(torch.float64).contiguous()
+
+
+def _scratch(nbytes: int, device) -> torch.Tensor:
+    return torch.empty(max(int(nbytes), 1), dtype=torch.uint8, device=device)
+
+
+class Topology:
+    """Node / edge order of a traversal list and, for the BP sweep, the
+    per-half-edge message sources and node levels that reproduce the
+    reference's sweep order exactly.
+
+    Asynchronous sweep (belief_propagation.py:39-45): elements are visited in
+    traversal order and read messages already updated in the same sweep.
+    For node v, bond to edge e with far end u:
+      * e after v                -> e2n from the previous sweep (SRC_E2N_OLD)
+      * e before v, u before e   -> u's node->edge message of this sweep (SRC_N2E_NEW)
+      * e before v, u after e    -> u's node->edge message of the previous sweep (SRC_N2E_OLD)
+    Nodes whose inputs are all available form a level; levels run in order.
+    The edge->node output of e toward v is u's node->edge message as it was
+    when e was visited (new iff u before e)."""
+
+    def __init__(self, traverser, is_synchronous: bool):
+        self.traverser = list(traverser)
+        self.nodes: List[Node] = [el for el in self.traverser if isinstance(el, Node)]
+        self.edges: List[Edge] = [el for el in self.traverser if isinstance(el, Edge)]
+        self.is_synchronous = is_synchronous
+        self.node_index = {n.id: i for i, n in enumerate(self.nodes)}
+        pos = {el.id: i for i, el in enumerate(self.traverser)}
+        degree = [len(n.neighbors) for n in self.nodes]
+        self.node_half = np.zeros(len(self.nodes), dtype=np.int64)
+        if self.nodes:
+            self.node_half[1:] = np.cumsum(degree)[:-1]
+        nh = int(sum(degree))
+        self.n_halves = nh
+        self.src_sel = np.zeros(nh, dtype=np.uint8)
+        self.edge_new = np.zeros(nh, dtype=np.uint8)
+        level = np.zeros(len(self.nodes), dtype=np.int64)
+        for v, nd in enumerate(self.nodes):
+            lv = 0
+            for slot, e in enumerate(nd.neighbors):
+                if e.degree != 2:
+                    raise NotImplementedError("BP on the GPU supports edges of degree 2 only")
+                u = e.neighbors[1] if e.neighbors[0] is nd else e.neighbors[0]
+                h = self.node_half[v] + slot
+                if u.id in pos and pos[u.id] < pos[e.id]:
+                    self.edge_new[h] = 1
+                if is_synchronous:
+                    self.src_sel[h] = _lib.SRC_E2N_OLD
+                    self.edge_new[h] = 0
+                elif pos[e.id] < pos[nd.id]:
+                    if pos[u.id] < pos[e.id]:
+                        self.src_sel[h] = _lib.SRC_N2E_NEW
+                        lv = max(lv, int(level[self.node_index[u.id]]) + 1)
+                    else:
+                        self.src_sel[h] = _lib.SRC_N2E_OLD
+                else:
+                    self.src_sel[h] = _lib.SRC_E2N_OLD
+            level[v] = lv
+        self.levels = []
+        if self.nodes:
+            for lv in range(int(level.max()) + 1):
+                vs = np.nonzero(level == lv)[0]
+                halves = np.concatenate([np.arange(self.node_half[v], self.node_half[v] + degree[v]) for v in vs])
+                self.levels.append(halves.astype(np.int32))
+        self._dev = None
+
+    def device_tables(self, device):
+        if self._dev is None:
+            self._dev = (
+                torch.from_numpy(self.src_sel).to(device),
+                torch.from_numpy(self.edge_new).to(device),
+                [torch.from_numpy(l).to(device) for l in self.levels],
+            )
+        return self._dev
+
+    def half_ids(self):
+        """(node, edge) element pairs of every half-edge, in half-edge order."""
+        return [(nd, e) for nd in self.nodes for e in nd.neighbors]
+
+
+class _LayoutCache:
+    def __init__(self, topo: Topology):
+        self.topo = topo
+        self._key = None
+        self._layout = None
+
+    def get(self, tensors) -> GraphLayout:
+        shapes = {n.id: tuple(tensors[n.id].shape) for n in self.topo.nodes}
+        key = tuple(shapes[n.id] for n in self.topo.nodes)
+        if key != self._key:
+            self._layout = layout_from_traverser(self.topo.traverser, shapes)
+            self._key = key
+        return self._layout
+
+
+def bp_sweep(layout: GraphLayout, topo: Topology, T, n2e_old, e2n_old, n2e_new, e2n_new):
+    """One sweep on packed arenas: node updates level by level, then the edge pass."""
+    src_sel, edge_new, levels = topo.device_tables(layout.device)
+    stream = _lib.stream_handle()
+    max_slice, max_chi = layout.max_slice(), layout.max_chi()
+    scratch = None
+    nbytes = _lib.lib().dqz_bp_node_scratch_bytes(max(len(l) for l in topo.levels), max_slice, max_chi)
+    if nbytes:
+        scratch = _scratch(nbytes, layout.device)
+    for halves in levels:
+        _lib.call(
+            "dqz_bp_node_update", layout.gptr, T.data_ptr(), n2e_old.data_ptr(), e2n_old.data_ptr(),
+            n2e_new.data_ptr(), src_sel.data_ptr(), halves.data_ptr(), halves.numel(), max_slice, max_chi,
+            _lib.ptr(scratch), stream,
+        )
+    _lib.call(
+        "dqz_bp_edge_pass", layout.gptr, n2e_old.data_ptr(), n2e_new.data_ptr(), edge_new.data_ptr(),
+        e2n_new.data_ptr(), max_chi, stream,
+    )
+
+
+def get_belief_propagation_map(traverser, is_synchronous: bool = False):
+    topo = Topology(traverser, is_synchronous)
+    cache = _LayoutCache(topo)
+    halves = topo.half_ids()
+
+    def belief_propagation_map(tensors: Dict, messages: Dict) -> Dict:
+        dev_t = {n.id: as_device(tensors[n.id]) for n in topo.nodes}
+        layout = cache.get(dev_t)
+        T = layout.pack_tensors([dev_t[n.id] for n in topo.nodes])
+        n2e_old = layout.pack_messages([as_device(messages[MessageID(nd.id, e.id)]) for nd, e in halves])
+        e2n_old = layout.pack_messages([as_device(messages[MessageID(e.id, nd.id)]) for nd, e in halves])
+        n2e_new = torch.empty_like(n2e_old)
+        e2n_new = torch.empty_like(e2n_old)
+        bp_sweep(layout, topo, T, n2e_old, e2n_old, n2e_new, e2n_new)
+        hidx = {(nd.id, e.id): h for h, (nd, e) in enumerate(halves)}
+        out = {}
+        for el in topo.traverser:
+            if isinstance(el, Node):
+                for e in el.neighbors:
+                    out[MessageID(el.id, e.id)] = layout.message_view(n2e_new, hidx[(el.id, e.id)])
+            else:
+                for nd in el.neighbors:
+                    out[MessageID(el.id, nd.id)] = layout.message_view(e2n_new, hidx[(nd.id, el.id)])
+        return out
+
+    return belief_propagation_map
+
+
+def messages_frob_distance(lhs: Dict, rhs: Dict) -> torch.Tensor:
+    n = len(lhs)
+    assert n == len(rhs), f"{n}, {len(rhs)}"
+    keys = list(lhs.keys())
+    a = [as_device(lhs[k]).reshape(-1) for k in keys]
+    b = [as_device(rhs[k]).reshape(-1) for k in keys]
+    sizes = np.array([x.numel() for x in a], dtype=np.int64)
+    off = np.zeros(n + 1, dtype=np.int64)
+    off[1:] = np.cumsum(sizes)
+    dev = a[0].device
+    A, B = torch.cat(a), torch.cat(b)
+    d_off = torch.from_numpy(off).to(dev)
+    partial = torch.empty(n, dtype=torch.float64, device=dev)
+    out = torch.empty((), dtype=torch.float64, device=dev)
+    _lib.call("dqz_segment_distance", A.data_ptr(), B.data_ptr(), d_off.data_ptr(), n, partial.data_ptr(),
+              out.data_ptr(), _lib.stream_handle())
+    return out
+
+
+def vidal_gauge_packed(layout: GraphLayout, T, n2e, eps: float):
+    """Vidal gauge on packed arenas: returns (Gamma arena, lambda arena)."""
+    stream = _lib.stream_handle()
+    max_chi = layout.max_chi()
+    orth = torch.empty(max(layout.msg_elems, 1), dtype=torch.complex128, device=layout.device)
+    lam = layout.new_lam_arena()
+    nb = _lib.lib().dqz_vidal_edges_scratch_bytes(layout.n_edges, max_chi)
+    scratch = _scratch(nb, layout.device) if nb else None
+    _lib.call("dqz_vidal_edges", layout.gptr, n2e.data_ptr(), float(eps), orth.data_ptr(), lam.data_ptr(), max_chi,
+              _lib.ptr(scratch), stream)
+    G = torch.empty_like(T)
+    ms = layout.max_size()
+    nb = _lib.lib().dqz_absorb_scratch_bytes(layout.n_nodes, ms)
+    scratch = _scratch(nb, layout.device) if nb else None
+    _lib.call("dqz_absorb", layout.gptr, T.data_ptr(), orth.data_ptr(), G.data_ptr(), ms, _lib.ptr(scratch), stream)
+    return G, lam
+
+
+def get_vidal_gauge_fixing_map(traverser, eps):
+    topo = Topology(traverser, True)
+    cache = _LayoutCache(topo)
+    halves = topo.half_ids()
+
+    def vidal_gauge_fixing_map(tensors: Dict, messages: Dict):
+        dev_t = {n.id: as_device(tensors[n.id]) for n in topo.nodes}
+        layout = cache.get(dev_t)
+        T = layout.pack_tensors([dev_t[n.id] for n in topo.nodes])
+        n2e = layout.pack_messages([as_device(messages[MessageID(nd.id, e.id)]) for nd, e in halves])
+        G, lam = vidal_gauge_packed(layout, T, n2e, float(eps))
+        gs = layout.unpack_tensors(G)
+        gauged = {n.id: gs[i] for i, n in enumerate(topo.nodes)}
+        lambdas = {e.id: layout.lambda_view(lam, i) for i, e in enumerate(topo.edges)}
+        return gauged, lambdas
+
+    return vidal_gauge_fixing_map
+
+
+def vidal_distance_packed(layout: GraphLayout, G, lam, eps: float) -> torch.Tensor:
+    partial = torch.empty(max(layout.n_halves, 1), dtype=torch.float64, device=layout.device)
+    out = torch.empty((), dtype=torch.float64, device=layout.device)
+    _lib.call("dqz_vidal_distance", layout.gptr, G.data_ptr(), lam.data_ptr(), float(eps), partial.data_ptr(),
+              out.data_ptr(), layout.max_chi(), _lib.stream_handle())
+    return out
+
+
+def get_vidal_gauge_distance_map(traverser, eps):
+    topo = Topology(traverser, True)
+    cache = _LayoutCache(topo)
+
+    def vidal_gauge_distance(tensors: Dict, lambdas: Dict) -> torch.Tensor:
+        dev_t = {n.id: as_device(tensors[n.id]) for n in topo.nodes}
+        layout = cache.get(dev_t)
+        G = layout.pack_tensors([dev_t[n.id] for n in topo.nodes])
+        lam = layout.pack_lambdas([as_device_real(lambdas[e.id]) for e in topo.edges])
+        return vidal_distance_packed(layout, G, lam, float(eps))
+
+    return vidal_gauge_distance
+
+
+def get_symmetric_gauge_fixing_map(traverser, eps):
+    topo = Topology(traverser, True)
+    cache = _LayoutCache(topo)
+
+    def symmetric_gauge(tensors: Dict, lambdas: Dict) -> Dict:
+        dev_t = {n.id: as_device(tensors[n.id]) for n in topo.nodes}
+        layout = cache.get(dev_t)
+        G = layout.pack_tensors([dev_t[n.id] for n in topo.nodes])
+        lam = layout.pack_lambdas([as_device_real(lambdas[e.id]) for e in topo.edges])
+        out = torch.empty_like(G)
+        _lib.call("dqz_symmetric_gauge", layout.gptr, G.data_ptr(), lam.data_ptr(), float(eps), out.data_ptr(),
+                  _lib.stream_handle())
+        ts = layout.unpack_tensors(out)
+        return {n.id: ts[i] for i, n in enumerate(topo.nodes)}
+
+    return symmetric_gauge
+
+
+def lambdas2messages(lambdas: Dict) -> Dict:
+    """diag(lambda) in both directions of every edge."""
+    messages = {}
+    for edge_id, lmbd in lambdas.items():
+        m = torch.diag(as_device_real(lmbd)).to(torch.complex128)
+        for node_id in edge_id:
+            messages[MessageID(src=edge_id, dst=node_id)] = m
+            messages[MessageID(src=node_id, dst=edge_id)] = m
+    return messages
+
+
+def get_one_side_density_matrix(node: Node, tensors: Dict, messages: Dict) -> torch.Tensor:
+    t = as_device(tensors[node.id])
+    if t.dim() - 1 != node.degree:
+        raise AssertionError(f"{node.degree}, {t.dim() - 1}")
+    layout = GraphLayout([node], list(node.neighbors), list(t.shape[:-1]), phys=[t.shape[-1]])
+    T = layout.pack_tensors([t])
+    e2n = layout.pack_messages([as_device(messages[MessageID(e.id, node.id)]) for e in node.neighbors])
+    return density_packed(layout, T, e2n, [0])[0]
+
+
+def density_packed(layout: GraphLayout, T, e2n, nodes: List[int]) -> torch.Tensor:
+    """rho for the listed node indices: tensor [len(nodes), d, d]."""
+    dev = layout.device
+    idx = torch.tensor(nodes, dtype=torch.int32, device=dev)
+    mp = _lib.MAX_PHYS
+    rho = torch.zeros((len(nodes), mp * mp), dtype=torch.complex128, device=dev)
+    ms = layout.max_size()
+    nb = _lib.lib().dqz_density_scratch_bytes(len(nodes), ms)
+    scratch = _scratch(nb, dev) if nb else None
+    _lib.call("dqz_density_matrices", layout.gptr, T.data_ptr(), e2n.data_ptr(), idx.data_ptr(), len(nodes),
+              rho.data_ptr(), ms, _lib.ptr(scratch), _lib.stream_handle())
+    d = int(layout.phys[nodes[0]]) if nodes else 2
+    return rho[:, : d * d].reshape(len(nodes), d, d)

@@ -1,0 +1,177 @@
+/*
+ * dqz.h -- C ABI of libdqz.so, the B200 (sm_100a) kernels behind the
+ * graph-tensor-network hot path of LuchnikovI/dequantizer.
+ *
+ * Conventions
+ *  - Complex numbers are interleaved (re, im) pairs: complex128 = 2 doubles,
+ *    complex64 = 2 floats, the memory layout of numpy / torch complex dtypes.
+ *  - Every pointer argument except `const dqz_graph_t *` is a DEVICE pointer.
+ *    The graph descriptor itself is a host struct whose members are device
+ *    pointers; it is read on the host at launch time.
+ *  - Every entry point enqueues work on `stream` and returns without
+ *    synchronising. The return value is a dqz_status_t: DQZ_OK, or an
+ *    argument / launch error detected on the host.
+ *  - Node tensors are row-major over (a_0, ..., a_{k-1}, s): bonds in the
+ *    node's neighbour order, physical index last
+ *    (dequantizer/src/graph/tensor_graph.py:188). A message between a node and
+ *    an edge of bond dimension chi is a chi x chi row-major matrix m[b][a]
+ *    contracted over its second index (dequantizer/src/tensor_ops.py:45).
+ *  - Half-edge h = node_half[v] + slot is bond `slot` of node v. Per half-edge
+ *    the state holds n2e[h] (node -> edge message) and e2n[h]
+ *    (edge -> node message).
+ */
+#ifndef DQZ_H
+#define DQZ_H
+
+#include <stdint.h>
+#include <cuda_runtime_api.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  DQZ_OK = 0,
+  DQZ_ERR_ARG = 1,          /* bad pointer / size / shape argument        */
+  DQZ_ERR_UNSUPPORTED = 2,  /* shape outside the kernels' supported range */
+  DQZ_ERR_CUDA = 3,         /* a CUDA launch or runtime call failed       */
+  DQZ_ERR_NOT_CONVERGED = 4,
+  DQZ_ERR_NONFINITE = 5
+} dqz_status_t;
+
+/* Supported ranges of the kernels (checked on the host before launch). */
+#define DQZ_MAX_DEGREE 8
+#define DQZ_MAX_CHI 64
+#define DQZ_MAX_PHYS 8
+
+/* Device-resident description of a packed tensor graph (all members are
+ * device pointers except the counts). Built by dequantizer_b200.layout. */
+typedef struct {
+  int32_t n_nodes;
+  int32_t n_edges;
+  int32_t n_halves;            /* half-edges = sum of node degrees; equals
+                                  2 * n_edges when every edge has both ends
+                                  in the layout                              */
+  const int32_t *node_degree;  /* [n_nodes]                                */
+  const int32_t *node_phys;    /* [n_nodes] physical dimension              */
+  const int32_t *node_half;    /* [n_nodes] first half-edge of the node      */
+  const int64_t *node_off;     /* [n_nodes] tensor offset (complex elements) */
+  const int32_t *half_node;    /* [2E]                                       */
+  const int32_t *half_edge;    /* [2E]                                       */
+  const int32_t *half_twin;    /* [2E] the other end's half-edge             */
+  const int64_t *half_msg_off; /* [2E] message offset (complex elements)     */
+  const int32_t *edge_half;    /* [2E] (half of neighbours[0], of neighbours[1]) */
+  const int64_t *edge_lam_off; /* [E] lambda offset (real elements)          */
+  int32_t *edge_chi;           /* [E] current bond dimension                 */
+} dqz_graph_t;
+
+/* Library / device information. */
+int dqz_version(void);
+int dqz_device_supported(int device); /* 1 when the device is sm_100 */
+
+/* ---- Belief propagation (dequantizer/src/mappings/belief_propagation.py:24-64,
+ *      dequantizer/src/tensor_ops.py:36-76) ---------------------------------- */
+
+/* Source of the incoming edge->node message for each half-edge. */
+#define DQZ_SRC_E2N_OLD 0  /* e2n_old[h]                                   */
+#define DQZ_SRC_N2E_OLD 1  /* n2e_old[twin(h)]  (edge already passed, twin node not yet) */
+#define DQZ_SRC_N2E_NEW 2  /* n2e_new[twin(h)]  (twin node updated earlier this sweep)   */
+
+/* Node update: for every half-edge listed in `halves` (n_halves of them),
+ * n2e_new[h] = pass_through_node output for bond h, with the k-1 incoming
+ * messages taken per `src_sel`. Replaces tensor_ops.py:36-60.
+ * `scratch` may be NULL when dqz_bp_node_scratch_bytes returns 0. */
+int dqz_bp_node_update(const dqz_graph_t *g, const void *tensors /*c128*/,
+                       const void *n2e_old, const void *e2n_old, void *n2e_new,
+                       const uint8_t *src_sel, const int32_t *halves, int32_t n_halves,
+                       int32_t max_slice, int32_t max_chi, void *scratch, cudaStream_t stream);
+size_t dqz_bp_node_scratch_bytes(int32_t n_halves, int32_t max_slice, int32_t max_chi);
+
+/* Edge pass (tensor_ops.py:70-76): e2n_new[h] = (edge_new[h] ? n2e_new : n2e_old)[twin(h)]
+ * for every half-edge. */
+int dqz_bp_edge_pass(const dqz_graph_t *g, const void *n2e_old, const void *n2e_new,
+                     const uint8_t *edge_new, void *e2n_new, int32_t max_chi, cudaStream_t stream);
+
+/* Mean Frobenius distance over all 4E messages (mappings/messages_distance.py:14-22):
+ * out[0] = (sum_h |n2e_a[h]-n2e_b[h]| + |e2n_a[h]-e2n_b[h]|) / (4E).
+ * `partial` is device scratch of 2*(2E) doubles. */
+int dqz_messages_distance(const dqz_graph_t *g, const void *n2e_a, const void *n2e_b,
+                          const void *e2n_a, const void *e2n_b, double *partial, double *out,
+                          int32_t max_chi, cudaStream_t stream);
+
+/* out[0] = scale * sum(partial[0..n)), deterministic single-CTA reduction. */
+int dqz_reduce_sum(const double *partial, int32_t n, double scale, double *out, cudaStream_t stream);
+
+/* out[0] = mean over i < n of |a[seg_off[i]:seg_off[i+1]] - b[...]|_F (complex128
+ * segments; messages_distance.py:14-22 over messages packed in one order).
+ * partial: n doubles of scratch. */
+int dqz_segment_distance(const void *a, const void *b, const int64_t *seg_off, int32_t n,
+                         double *partial, double *out, cudaStream_t stream);
+
+/* Copies n segments: dst[dst_off[i] .. + count[i]) = src[src_off[i] .. + count[i]),
+ * offsets and counts in elements of elem_bytes (8 or 16). Used to move node
+ * tensors / lambdas into a layout with larger capacities. */
+int dqz_repack(const void *src, void *dst, const int64_t *src_off, const int64_t *dst_off,
+               const int64_t *count, int32_t n, int32_t elem_bytes, cudaStream_t stream);
+
+/* ---- Vidal gauge (mappings/vidal_gauge.py:21-63, tensor_ops.py:88-130) ---- */
+
+/* Per edge: eigendecompose both node->edge messages, build sqrt / safe inverse
+ * sqrt, SVD of sqrt(m_f) sqrt(m_b)^T; write lambdas and the two
+ * orthogonalisers orth[h] (chi x chi, complex128, at half_msg_off[h]). */
+int dqz_vidal_edges(const dqz_graph_t *g, const void *n2e, double eps, void *orth,
+                    double *lambdas, int32_t max_chi, void *scratch, cudaStream_t stream);
+size_t dqz_vidal_edges_scratch_bytes(int32_t n_edges, int32_t max_chi);
+/* Per node: T_out = T x_e orth[h_e] over every bond (bond index contracted
+ * with the row index), normalised. */
+int dqz_absorb(const dqz_graph_t *g, const void *tensors_in, const void *orth, void *tensors_out,
+               int32_t max_size, void *scratch, cudaStream_t stream);
+size_t dqz_absorb_scratch_bytes(int32_t n_nodes, int32_t max_size);
+
+/* ---- Vidal distance (mappings/vidal_distance.py:17-42, tensor_ops.py:143-175) */
+int dqz_vidal_distance(const dqz_graph_t *g, const void *tensors, const double *lambdas,
+                       double eps, double *partial /*[2E]*/, double *out,
+                       int32_t max_chi, cudaStream_t stream);
+
+/* ---- Symmetric gauge (mappings/symmetric_gauge.py:17-61, tensor_ops.py:189-199) */
+int dqz_symmetric_gauge(const dqz_graph_t *g, const void *tensors_in, const double *lambdas,
+                        double eps, void *tensors_out, cudaStream_t stream);
+int dqz_lambdas_to_messages(const dqz_graph_t *g, const double *lambdas, void *n2e, void *e2n,
+                            int32_t max_chi, cudaStream_t stream);
+
+/* ---- One-site density matrices (mappings/density_matrix.py:16-37) ---------- */
+/* rho[v] (d x d, complex128, at v * DQZ_MAX_PHYS^2) for every node in `nodes`. */
+int dqz_density_matrices(const dqz_graph_t *g, const void *tensors, const void *e2n,
+                         const int32_t *nodes, int32_t n_nodes, void *rho,
+                         int32_t max_size, void *scratch, cudaStream_t stream);
+size_t dqz_density_scratch_bytes(int32_t n_nodes, int32_t max_size);
+
+/* ---- Gates (tensor_graph.py:268-446, tensor_ops.py:202-389) --------------- */
+
+/* apply1 (tensor_graph.py:268-275) on n distinct nodes: T[..., o] = sum_i T[..., i] G[o, i],
+ * normalised, in place. gates: n x d x d complex128. */
+int dqz_apply1(const dqz_graph_t *g, void *tensors, const int32_t *nodes, const void *gates,
+               int32_t n, cudaStream_t stream);
+
+/* apply2 halves (tensor_ops.py:221-262): out tensor with bond `slot` grown by r.
+ * One launch handles n (node, slot, half) jobs; in/out offsets per job. */
+int dqz_apply_half_gates(const void *tensors_in, void *tensors_out, const int64_t *in_off,
+                         const int64_t *out_off, const int32_t *shape /*n x (DQZ_MAX_DEGREE+2)*/,
+                         const void *halves /*n x 4 x d x d*/, int32_t n, cudaStream_t stream);
+
+/* Simple update (tensor_ops.py:265-389) for n node-disjoint edges in parallel.
+ * For job j: edge edges[j], controlling node = endpoint `first_is_ctrl[j] ? 0 : 1`,
+ * halves = halves[j] (2 x 4 x d x d: controlling then controlled, rank[j] rows used).
+ * Writes Gamma tensors in place (capacity layout), lambdas, edge_chi, and
+ * err/entropy per job. */
+int dqz_simple_update(const dqz_graph_t *g, void *tensors, double *lambdas,
+                      const int32_t *edges, const uint8_t *ctrl_is_first, const void *halves,
+                      const int32_t *ranks, int32_t n, double eps, int32_t max_rank,
+                      int32_t max_rows, int32_t max_cols, double *err, double *entropy,
+                      void *scratch, cudaStream_t stream);
+size_t dqz_simple_update_scratch_bytes(int32_t n, int32_t max_rows, int32_t max_cols);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DQZ_H */

@@ -1,0 +1,178 @@
+"""GPU parity of the dict-interface maps against the FP64 oracle.
+
+Tolerances (FP64 kernels vs numpy/LAPACK): 1e-11 relative for direct outputs
+(messages, symmetric-gauge tensors, density matrices, gates), 1e-10 for
+spectra and gauge-invariant contractions that pass through eigen/SVD solvers.
+"""
+
+import numpy as np
+import pytest
+import torch
+
+from dequantizer_b200 import graph as G
+from dequantizer_b200 import maps as M
+from dequantizer_b200.graph import MessageID, Node
+from oracle import maps as OM
+from oracle import tensor_ops as OT
+from tests.helpers import (contract_network, random_messages, random_tensors, rel_err, state_fidelity, to_np,
+                           two_site)
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-11
+TOL_SVD = 1e-10
+
+
+def graphs():
+    yield "tree_d3", G.get_random_tree_tensor_graph(9, 3, [2, 3, 4], 5)
+    yield "lattice_2x3x2", G.get_nd_lattice([2, 3, 2], 2, 2)
+    yield "regular_3", G.get_random_regular_graph(8, 3, 2, 3, 11)
+    yield "eagle_cell", G.get_heavy_hex_ibm_eagle_lattice_infinite()
+
+
+@pytest.mark.parametrize("sync", [True, False])
+@pytest.mark.parametrize("ordering", ["dfs", "bfs"])
+@pytest.mark.parametrize("case", list(graphs()), ids=lambda c: c[0])
+def test_bp_sweep_matches_oracle(case, ordering, sync):
+    name, g = case
+    if name == "eagle_cell":
+        for e in g.edges.values():
+            e.dimension = 3
+        g.refresh_bond_shapes()
+    trav = list(g.get_traversal_iterator(ordering=ordering))
+    tensors = random_tensors(g, 1)
+    messages = random_messages(g, 2)
+    ref = OM.get_belief_propagation_map(trav, sync)
+    gpu = M.get_belief_propagation_map(trav, sync)
+    r_msgs, g_msgs = messages, messages
+    for _ in range(3):
+        r_msgs = ref(tensors, r_msgs)
+        g_msgs = gpu(tensors, g_msgs)
+        assert list(r_msgs.keys()) == list(g_msgs.keys())
+        for k in r_msgs:
+            assert rel_err(g_msgs[k], r_msgs[k]) < TOL, (k, rel_err(g_msgs[k], r_msgs[k]))
+    d_ref = OM.messages_frob_distance(r_msgs, messages)
+    d_gpu = float(M.messages_frob_distance(g_msgs, messages))
+    assert abs(d_ref - d_gpu) < 1e-10 * max(1.0, d_ref)
+
+
+def _converged_messages(g, tensors, n=200, tol=1e-13):
+    trav = list(g.get_traversal_iterator())
+    bp = OM.get_belief_propagation_map(trav)
+    msgs = random_messages(g, 3)
+    for _ in range(n):
+        new = bp(tensors, msgs)
+        d = OM.messages_frob_distance(new, msgs)
+        msgs = new
+        if d < tol:
+            break
+    return trav, msgs
+
+
+@pytest.mark.parametrize("case", list(graphs())[:3], ids=lambda c: c[0])
+def test_vidal_gauge_matches_oracle(case):
+    name, g = case
+    tensors = random_tensors(g, 4)
+    trav, msgs = _converged_messages(g, tensors)
+    eps = 1e-10
+    r_t, r_l = OM.get_vidal_gauge_fixing_map(trav, eps)(tensors, msgs)
+    g_t, g_l = M.get_vidal_gauge_fixing_map(trav, eps)(tensors, msgs)
+    for eid in r_l:
+        assert rel_err(g_l[eid], r_l[eid]) < TOL_SVD
+    for nid in r_t:
+        assert abs(np.linalg.norm(to_np(g_t[nid])) - 1.0) < 1e-12
+    # the Vidal form contracts (with lambdas on the bonds) to the same state
+    psi_ref = contract_network(g, r_t, r_l)
+    psi_gpu = contract_network(g, g_t, g_l)
+    assert 1.0 - state_fidelity(psi_ref, psi_gpu) < 1e-10
+    # Vidal distance of the GPU gauge, by the GPU and by the oracle
+    vd_gpu = float(M.get_vidal_gauge_distance_map(trav, eps)(g_t, g_l))
+    vd_orc = OM.get_vidal_gauge_distance_map(trav, eps)({k: to_np(v) for k, v in g_t.items()},
+                                                        {k: to_np(v) for k, v in g_l.items()})
+    assert abs(vd_gpu - vd_orc) < 1e-10
+
+
+@pytest.mark.parametrize("case", list(graphs())[:3], ids=lambda c: c[0])
+def test_symmetric_gauge_density_and_lambdas(case):
+    name, g = case
+    tensors = random_tensors(g, 6)
+    rng = np.random.default_rng(7)
+    lambdas = {eid: np.sort(rng.uniform(0, 1, e.dimension))[::-1].copy() for eid, e in g.edges.items()}
+    trav = list(g.get_traversal_iterator())
+    r = OM.get_symmetric_gauge_fixing_map(trav, 1e-10)(tensors, lambdas)
+    s = M.get_symmetric_gauge_fixing_map(trav, 1e-10)(tensors, lambdas)
+    for nid in r:
+        assert rel_err(s[nid], r[nid]) < TOL
+    rm = OM.lambdas2messages(lambdas)
+    gm = M.lambdas2messages(lambdas)
+    for k in rm:
+        assert rel_err(gm[k], rm[k]) < TOL
+    msgs = random_messages(g, 8)
+    for el in trav:
+        if isinstance(el, Node):
+            a = OM.get_one_side_density_matrix(el, tensors, msgs)
+            b = M.get_one_side_density_matrix(el, tensors, msgs)
+            assert rel_err(b, a) < TOL
+
+
+def test_vidal_distance_matches_oracle():
+    g = G.get_nd_lattice([3, 2, 2], 2, 3)
+    tensors = random_tensors(g, 9)
+    rng = np.random.default_rng(10)
+    lambdas = {eid: rng.uniform(0.1, 1, e.dimension) for eid, e in g.edges.items()}
+    trav = list(g.get_traversal_iterator())
+    a = OM.get_vidal_gauge_distance_map(trav, 1e-10)(tensors, lambdas)
+    b = float(M.get_vidal_gauge_distance_map(trav, 1e-10)(tensors, lambdas))
+    assert abs(a - b) < 1e-10 * max(1.0, a)
+
+
+def test_apply1_apply2_match_oracle():
+    g_ref = G.get_nd_lattice([2, 3], 2, 2)
+    g_gpu = G.get_nd_lattice([2, 3], 2, 2)
+    tensors = random_tensors(g_ref, 12)
+    rng = np.random.default_rng(13)
+    r_t = dict(tensors)
+    g_t = dict(tensors)
+    gate1 = rng.standard_normal((2, 2)) + 1j * rng.standard_normal((2, 2))
+    OM.apply1(g_ref, (0, 0), r_t, gate1)
+    g_gpu.apply1((0, 0), g_t, gate1)
+    assert rel_err(g_t[(0, 0)], r_t[(0, 0)]) < TOL
+    cnot = np.array([[1, 0, 0, 0], [0, 1, 0, 0], [0, 0, 0, 1], [0, 0, 1, 0]], dtype=np.complex128).reshape(2, 2, 2, 2)
+    for a, b in [((0, 0), (0, 1)), ((1, 1), (0, 1)), ((0, 2), (1, 2))]:
+        OM.apply2(g_ref, a, b, r_t, cnot, 1e-8)
+        g_gpu.apply2(a, b, g_t, cnot, 1e-8)
+    for nid in r_t:
+        assert tuple(g_t[nid].shape) == r_t[nid].shape
+        assert rel_err(g_t[nid], r_t[nid]) < TOL
+    for eid in g_ref.edges:
+        assert g_ref.get_edge(eid).dimension == g_gpu.get_edge(eid).dimension
+
+
+@pytest.mark.parametrize("max_rank", [None, 3, 6])
+@pytest.mark.parametrize("accuracy", [None, 1e-3])
+def test_simple_update_matches_oracle(max_rank, accuracy):
+    g_ref = G.get_random_regular_graph(8, 3, 2, 4, 21)
+    g_gpu = G.get_random_regular_graph(8, 3, 2, 4, 21)
+    tensors = random_tensors(g_ref, 14)
+    rng = np.random.default_rng(15)
+    lambdas = {eid: np.sort(rng.uniform(0.05, 1, e.dimension))[::-1].copy() for eid, e in g_ref.edges.items()}
+    gate = np.diag(np.exp(1j * rng.standard_normal(4))).reshape(2, 2, 2, 2)
+    z = rng.standard_normal((4, 4, 2))
+    u, _ = np.linalg.qr(z[..., 0] + 1j * z[..., 1])
+    gate_full = u.reshape(2, 2, 2, 2)
+    r_t, r_l = dict(tensors), dict(lambdas)
+    g_t, g_l = dict(tensors), dict(lambdas)
+    for gt, (a, b) in [(gate, list(g_ref.edges)[0]), (gate_full, list(g_ref.edges)[3]), (gate, list(g_ref.edges)[5])]:
+        _, _, er, en = OM.apply2_to_vidal_canonical(g_ref, a, b, r_t, r_l, gt, 1e-10, accuracy, max_rank)
+        _, _, eg, ng = g_gpu.apply2_to_vidal_canonical(a, b, g_t, g_l, gt, 1e-10, accuracy, max_rank)
+        edge = g_ref.find_edge(a, b)
+        assert g_gpu.find_edge(a, b).dimension == edge.dimension
+        assert rel_err(g_l[edge.id], r_l[edge.id]) < TOL_SVD
+        assert abs(float(eg) - er) < 1e-10
+        assert abs(float(ng) - en) < 1e-10
+        n1, n2 = g_ref.get_node(a), g_ref.get_node(b)
+        th_r = two_site(r_t[a], r_t[b], n1.indices[edge.id], n2.indices[edge.id], r_l[edge.id])
+        th_g = two_site(g_t[a], g_t[b], n1.indices[edge.id], n2.indices[edge.id], g_l[edge.id])
+        assert rel_err(th_g, th_r) < TOL_SVD
+        # bring the GPU state back to the oracle's so later gates see identical inputs
+        g_t[a], g_t[b], g_l[edge.id] = r_t[a], r_t[b], r_l[edge.id]
