@@ -1,0 +1,355 @@
+"""Benchmark: BP edge-updates/s on a random 3-regular graph (1024 nodes,
+bond dimension 16, physical dimension 2), one GPU per rank.
+
+A step is one full BP sweep over every directed edge (3072 edge-updates) in
+the reference's synchronous mode (one node-update launch + one edge pass).
+``value`` is timed on the device with CUDA events per step, inputs resident
+in HBM, L2 flushed (a 512 MB write) between steps outside the timed events.
+``e2e`` is the same sweep through the public engine API with host buffers:
+pinned complex64 node tensors and complex128 messages copied in, the sweep,
+the node->edge messages copied back, all inside the timed region.
+
+``--impl reference`` times the CPU restatement of the reference algorithm
+(numpy FP64, threads over nodes) on a bounded sample of the same workload.
+With torchrun (N > 1) every rank runs an independent replica ("replicas
+only": the sweep of one graph has no exchange step here).
+"""
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "BP edge-updates/s & anneal steps/s vs plain FP64 on GPU at |Δ<Z>|≤1e-4"
+UNIT = "edge-updates/s"
+N_NODES, DEGREE, CHI, PHYS, SEED = 1024, 3, 16, 2, 0
+
+
+def workload(rank: int = 0):
+    """Graph, complex64 node tensors (node order of the DFS traversal) and
+    PSD messages (half-edge order), seeded."""
+    from dequantizer_b200.graph import get_random_regular_graph
+
+    g = get_random_regular_graph(N_NODES, DEGREE, PHYS, CHI, SEED + rank)
+    rng = np.random.default_rng(1000 + rank)
+    size = CHI**DEGREE * PHYS
+    scale = 1.0 / np.sqrt(2.0 * CHI**DEGREE)
+    z = rng.standard_normal((N_NODES, size, 2), dtype=np.float32)
+    tensors = ((z[..., 0] + 1j * z[..., 1]) * (scale / np.sqrt(2.0))).astype(np.complex64)
+    a = rng.standard_normal((CHI, CHI, 2))
+    a = a[..., 0] + 1j * a[..., 1]
+    m = a @ a.conj().T
+    m /= np.trace(m).real
+    return g, tensors, m
+
+
+def flops_per_edge_update(k=DEGREE, d=PHYS, chi=CHI):
+    return 8 * k * d * chi ** (k + 1)
+
+
+def bytes_per_edge_update(k=DEGREE, d=PHYS, chi=CHI, s=16):
+    return s * (d * chi**k + 2 * k * chi * chi) / k
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx.append(float(p[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, p[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(mx)), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup():
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    elif torch.cuda.is_available():
+        torch.cuda.set_device(0)
+    return world, rank, local
+
+
+def reduce_max(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def measure_fp64_peak(torch):
+    """cuBLAS DGEMM throughput (best of 3, 8192^3), the FP64 roofline."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 1e30
+    for _ in range(3):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        torch.matmul(a, b)
+        e.record()
+        e.synchronize()
+        best = min(best, s.elapsed_time(e) * 1e-3)
+    del a, b
+    return 2.0 * n**3 / best / 1e12
+
+
+def cpu_baseline_sample(g, tensors_c64, m, seconds=12.0, threads=None):
+    """Oracle pass_through_node over nodes (threads over nodes), on the host
+    cores, for about ``seconds``; returns (edge-updates/s, threads, sample)."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    from oracle import tensor_ops as OT
+
+    threads = threads or os.cpu_count() or 1
+    nodes = list(g.nodes.values())
+    shape = (CHI,) * DEGREE + (PHYS,)
+    msgs = [m] * DEGREE
+
+    def work(v):
+        OT.pass_through_node(tensors_c64[v].astype(np.complex128).reshape(shape), msgs)
+        return DEGREE
+
+    done, t0, v = 0, time.perf_counter(), 0
+    with ThreadPoolExecutor(max_workers=threads) as ex:
+        while time.perf_counter() - t0 < seconds:
+            batch = [(v + i) % len(nodes) for i in range(threads * 4)]
+            v += len(batch)
+            done += sum(ex.map(work, batch))
+    dt = time.perf_counter() - t0
+    return done / dt, threads, f"{done} edge-updates ({done // DEGREE} nodes' pass_through_node) in {dt:.1f}s"
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    g, tensors, m = workload(0)
+    for _ in range(args.warmup):
+        cpu_baseline_sample(g, tensors, m, seconds=1.0)
+    vals = []
+    for _ in range(args.steps):
+        v, threads, sample = cpu_baseline_sample(g, tensors, m, seconds=args.ref_seconds)
+        vals.append(v)
+    value = float(np.mean(vals))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 3 * N_NODES / value * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+        "config": {"workload": "random 3-regular graph, 1024 nodes, chi=16, d=2: one synchronous BP sweep "
+                   "(3072 edge-updates)", "sample_per_step": f"~{args.ref_seconds:.0f}s of node updates"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": "numpy FP64 restatement of tensor_ops.pass_through_node, threads over nodes, "
+                                   + sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, world, rank, local):
+    import torch
+
+    from dequantizer_b200.engine import BPEngine
+
+    g, tensors, m = workload(rank)
+    eng = BPEngine(g, traversal="dfs", schedule="sync")
+    L = eng.layout
+    # engine node order is the traversal order: permute once on the host
+    node_ids = list(g.nodes.keys())
+    pos = {nid: i for i, nid in enumerate(node_ids)}
+    perm = np.array([pos[n.id] for n in eng.topo.nodes])
+    packed_c64 = torch.from_numpy(np.ascontiguousarray(tensors[perm]).reshape(-1)).pin_memory()
+    n2e_host = torch.from_numpy(np.tile(m.reshape(-1), L.n_halves)).pin_memory()
+    e2n_host = n2e_host.clone().pin_memory()
+    out_host = torch.empty_like(n2e_host).pin_memory()
+    eng.load_tensors_host(packed_c64)
+    eng.load_messages_host(n2e_host, e2n_host)
+    torch.cuda.synchronize()
+    edge_updates = L.n_halves
+    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    stream = torch.cuda.current_stream()
+
+    # warm-up
+    for _ in range(args.warmup):
+        eng.sweep()
+    torch.cuda.synchronize()
+
+    # ---- device-timed sweeps (inputs resident, L2 flushed between steps)
+    barrier(world)
+    torch.cuda.synchronize()
+    times, node_times = [], []
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            flush.zero_()
+            e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+            e0.record(stream)
+            eng.sweep(mid_event=e1)
+            e2.record(stream)
+            e2.synchronize()
+            times.append(e0.elapsed_time(e2) * 1e-3)
+            node_times.append(e0.elapsed_time(e1) * 1e-3)
+    torch.cuda.synchronize()
+    barrier(world)
+    total = reduce_max(sum(times), world)
+    value = world * edge_updates * args.steps / total
+    node_avg = float(np.mean(node_times))
+
+    # ---- end to end: host buffers in, sweep, messages out
+    barrier(world)
+    torch.cuda.synchronize()
+    e_times = []
+    for _ in range(args.steps):
+        flush.zero_()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        eng.load_tensors_host(packed_c64)
+        eng.load_messages_host(n2e_host, e2n_host)
+        eng.sweep()
+        eng.read_messages_host(out_host)
+        e.record(stream)
+        e.synchronize()
+        e_times.append(s.elapsed_time(e) * 1e-3)
+    e_total = reduce_max(sum(e_times), world)
+    e2e_value = world * edge_updates * args.steps / e_total
+    h2d = packed_c64.numel() * 8 + 2 * n2e_host.numel() * 16
+    d2h = out_host.numel() * 16
+
+    peak = measure_fp64_peak(torch) if rank == 0 else None
+    if rank != 0:
+        return
+    fl = flops_per_edge_update() * edge_updates
+    achieved = fl / node_avg / 1e12
+    traffic = None
+    tfile = os.path.join(ROOT, "profiles", "bp_node_generic_rr1024_chi16.traffic.json")
+    if os.path.exists(tfile):
+        with open(tfile) as f:
+            traffic = json.load(f).get("dram_bytes_per_launch")
+    cpu_v, cores, sample = (None, None, None)
+    if world == 1 and not args.no_cpu:
+        cpu_v, cores, sample = cpu_baseline_sample(g, tensors, m, seconds=args.cpu_seconds)
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total / args.steps * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+        "config": {
+            "workload": "random 3-regular graph (pairing model, seed 0), 1024 nodes, chi=16, d=2, complex64 "
+                        "inputs upcast to complex128: one synchronous BP sweep = 3072 edge-updates per step",
+            "precision": "fp64 (complex128)", "schedule": "reference synchronous sweep",
+            "l2": "flushed between steps (512 MB write)", "parallelism": f"replicas x{world}",
+        },
+        "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                     "frac": achieved / peak if peak else None, "traffic": traffic,
+                     "kernel": "bp_node_generic", "peak_source": "cuBLAS DGEMM 8192^3 measured in this run",
+                     "flops_per_launch": fl, "launch_ms": node_avg * 1e3},
+        "cpu_baseline": {"value": cpu_v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "gpu_launches": eng.launches_per_sweep() * args.steps,
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--ref-seconds", type=float, default=8.0)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        world = int(os.environ.get("WORLD_SIZE", "1"))
+        rank = int(os.environ.get("RANK", "0"))
+        run_reference(args, world, rank)
+        return
+    world, rank, local = dist_setup()
+    try:
+        run_ours(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -73,8 +73,9 @@ class Topology:
     The edge->node output of e toward v is u's node->edge message as it was
     when e was visited (new iff u before e)."""
 
-    def __init__(self, traverser, is_synchronous: bool):
+    def __init__(self, traverser, is_synchronous: bool, flooding: bool = False):
         self.traverser = list(traverser)
+        self.flooding = flooding
         self.nodes: List[Node] = [el for el in self.traverser if isinstance(el, Node)]
         self.edges: List[Edge] = [el for el in self.traverser if isinstance(el, Edge)]
         self.is_synchronous = is_synchronous
@@ -98,7 +99,12 @@ class Topology:
                 h = self.node_half[v] + slot
                 if u.id in pos and pos[u.id] < pos[e.id]:
                     self.edge_new[h] = 1
-                if is_synchronous:
+                if flooding:
+                    # every node reads the far end's node->edge message of the
+                    # previous sweep; edges forward this sweep's messages
+                    self.src_sel[h] = _lib.SRC_N2E_OLD
+                    self.edge_new[h] = 1
+                elif is_synchronous:
                     self.src_sel[h] = _lib.SRC_E2N_OLD
                     self.edge_new[h] = 0
                 elif pos[e.id] < pos[nd.id]:
