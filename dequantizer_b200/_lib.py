@@ -95,6 +95,7 @@ _SIGNATURES = {
     "dqz_apply_half_gates": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _I, _P]),
     "dqz_simple_update": (ctypes.c_int, [_G, _P, _P, _P, _P, _P, _P, _I, _D, _I, _I, _I, _P, _P, _P, _P]),
     "dqz_simple_update_scratch_bytes": (_S, [_I, _I, _I]),
+    "dqz_simple_update_noalloc": (ctypes.c_int, [_G, _P, _P, _P, _P, _P, _P, _I, _D, _I, _I, _I, _P, _P, _P]),
     "dqz_repack": (ctypes.c_int, [_P, _P, _P, _P, _P, _I, _I, _P]),
 }
 

@@ -377,3 +377,67 @@ extern "C" int dqz_simple_update(const dqz_graph_t *g, void *tensors, double *la
   DQZ_CHECK_LAUNCH();
   return DQZ_OK;
 }
+
+// ------------------------------------------- simple update, no allocation
+// Scratch for dqz_simple_update_noalloc. It is part of the library image, so
+// every GPU that loads libdqz keeps these bytes until the process exits. In
+// host code `noalloc_scratch` only names a host-side stand-in: device code
+// receives the address that cudaGetSymbolAddress returns for the current
+// device.
+static __device__ __align__(256) unsigned char noalloc_scratch[DQZ_NOALLOC_SCRATCH_BYTES];
+
+#include <mutex>
+
+namespace {
+
+constexpr int NOALLOC_MAX_DEVICES = 64;
+std::mutex noalloc_mutex;
+void *noalloc_ptr[NOALLOC_MAX_DEVICES] = {nullptr};
+
+// Device address of noalloc_scratch on the current device, looked up once
+// per device (the first call on a device does this).
+int noalloc_address(void **out) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return DQZ_ERR_CUDA;
+  if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return DQZ_ERR_UNSUPPORTED;
+  std::lock_guard<std::mutex> lock(noalloc_mutex);
+  if (!noalloc_ptr[dev]) {
+    void *p = nullptr;
+    if (cudaGetSymbolAddress(&p, noalloc_scratch) != cudaSuccess || !p) return DQZ_ERR_CUDA;
+    noalloc_ptr[dev] = p;
+  }
+  *out = noalloc_ptr[dev];
+  return DQZ_OK;
+}
+
+}  // namespace
+
+extern "C" int dqz_simple_update_noalloc(const dqz_graph_t *g, void *tensors, double *lambdas, const int32_t *edges,
+                                         const uint8_t *ctrl_is_first, const void *halves, const int32_t *ranks,
+                                         int32_t n, double eps, int32_t max_rank, int32_t max_rows, int32_t max_cols,
+                                         double *err, double *entropy, cudaStream_t stream) {
+  if (!g || !tensors || !lambdas || !edges || !ctrl_is_first || !halves || !ranks || !err || !entropy)
+    return DQZ_ERR_ARG;
+  if (n < 0 || max_rows <= 0 || max_cols <= 0) return DQZ_ERR_ARG;
+  if (max_cols > DQZ_MAX_CHI) return DQZ_ERR_UNSUPPORTED;
+  const size_t per_job = su_scratch_per_job(max_rows, max_cols);
+  if (per_job > (size_t)DQZ_NOALLOC_SCRATCH_BYTES) return DQZ_ERR_UNSUPPORTED;
+  if (n == 0) return DQZ_OK;
+  const size_t smem = su_smem_bytes(max_cols);
+  if (smem > SMEM_LIMIT) return DQZ_ERR_UNSUPPORTED;
+  void *scratch = nullptr;
+  const int st = noalloc_address(&scratch);
+  if (st != DQZ_OK) return st;
+  // as many CTAs as job scratch slices fit in the array; each CTA loops over jobs
+  size_t slots = (size_t)DQZ_NOALLOC_SCRATCH_BYTES / per_job;
+  int grid = n < SU_GRID_MAX ? n : SU_GRID_MAX;
+  if ((size_t)grid > slots) grid = (int)slots;
+  if (cudaFuncSetAttribute(simple_update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_LIMIT) !=
+      cudaSuccess)
+    return DQZ_ERR_CUDA;
+  simple_update_kernel<<<grid, GATE_THREADS, smem, stream>>>(*g, (cd *)tensors, lambdas, edges, ctrl_is_first,
+                                                             (const cd *)halves, ranks, n, eps, max_rank, max_rows,
+                                                             max_cols, err, entropy, (cd *)scratch);
+  DQZ_CHECK_LAUNCH();
+  return DQZ_OK;
+}

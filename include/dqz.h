@@ -171,6 +171,34 @@ int dqz_simple_update(const dqz_graph_t *g, void *tensors, double *lambdas,
                       void *scratch, cudaStream_t stream);
 size_t dqz_simple_update_scratch_bytes(int32_t n, int32_t max_rows, int32_t max_cols);
 
+/* Size of the library-owned scratch array behind dqz_simple_update_noalloc. */
+#define DQZ_NOALLOC_SCRATCH_BYTES (32u << 20) /* 32 MiB */
+
+/* dqz_simple_update without a scratch argument and without any device
+ * allocation. No counterpart in the reference: it exists for callers that
+ * cannot allocate device memory themselves -- for example a host program that
+ * hands this library only its input and output buffers from a pool it manages
+ * under a fixed memory budget, or a latency-bound loop that cannot afford the
+ * implicit device synchronisation of cudaMalloc / cudaFree.
+ *  - The scratch is a DQZ_NOALLOC_SCRATCH_BYTES (32 MiB) array compiled into
+ *    the library; every GPU that loads the library holds it until the process
+ *    exits. One job needs 64 * max_rows * max_cols bytes; a call whose job
+ *    needs more returns DQZ_ERR_UNSUPPORTED. Jobs beyond the number of slices
+ *    that fit run one after another inside the launch.
+ *  - The first call on each device looks up the array's device address
+ *    (cudaGetSymbolAddress with that device current); make that first call
+ *    before any stream capture.
+ *  - Every call uses the same array and it keeps whatever the last call left
+ *    there (the kernel writes every scratch word before reading it). Calls
+ *    whose kernels overlap on the GPU -- on different streams, or from
+ *    different host threads -- race on the array; serialise them.
+ * Arguments and results are those of dqz_simple_update. */
+int dqz_simple_update_noalloc(const dqz_graph_t *g, void *tensors, double *lambdas,
+                              const int32_t *edges, const uint8_t *ctrl_is_first, const void *halves,
+                              const int32_t *ranks, int32_t n, double eps, int32_t max_rank,
+                              int32_t max_rows, int32_t max_cols, double *err, double *entropy,
+                              cudaStream_t stream);
+
 #ifdef __cplusplus
 }
 #endif
