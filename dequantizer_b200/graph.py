@@ -431,19 +431,58 @@ def get_random_regular_graph(
 
 
 def greedy_edge_coloring(graph: TensorGraph) -> List[List[EdgeID]]:
-    """Splits edges into classes of node-disjoint edges (a proper edge
-    colouring), assigning each edge, in insertion order, the smallest colour
-    not used at either endpoint."""
-    used: Dict[NodeID, Set[int]] = {nid: set() for nid in graph.nodes}
-    classes: List[List[EdgeID]] = []
+    """Splits the (two-node) edges into classes of node-disjoint edges.
+
+    Edges are coloured in insertion order with colours 0..D-1, D the maximum
+    degree. When no colour is free at both ends, the alternating a/b path
+    from one end (a free at u, b free at v) is recoloured b/a, which frees a
+    at v (Kempe chain). On bipartite graphs (heavy-hex, trees, open lattices)
+    this always succeeds, so D classes suffice (Konig's edge-colouring
+    theorem); when the path closes on an odd cycle a new colour is opened."""
+    at: Dict[NodeID, Dict[int, EdgeID]] = {nid: {} for nid in graph.nodes}
+    colour: Dict[EdgeID, int] = {}
+    n_colours = max((n.degree for n in graph.nodes.values()), default=0)
+
+    def other(eid, x):
+        a, b = eid
+        return b if x == a else a
+
     for eid, edge in graph.edges.items():
-        ends = [n.id for n in edge.neighbors]
-        c = 0
-        while any(c in used[n] for n in ends):
-            c += 1
-        for n in ends:
-            used[n].add(c)
-        while len(classes) <= c:
-            classes.append([])
-        classes[c].append(eid)
-    return classes
+        if edge.degree != 2:
+            raise NotImplementedError("edge colouring needs edges of degree 2")
+        u, v = eid
+        free_u = [c for c in range(n_colours) if c not in at[u]]
+        free_v = [c for c in range(n_colours) if c not in at[v]]
+        common = [c for c in free_u if c not in at[v]]
+        if common:
+            c = common[0]
+        elif free_u and free_v:
+            a, b = free_u[0], free_v[0]
+            path, x, want = [], v, a
+            while want in at[x]:
+                e = at[x][want]
+                path.append(e)
+                x = other(e, x)
+                want = b if want == a else a
+            if x == u or any(u in e for e in path):
+                c = n_colours
+                n_colours += 1
+            else:
+                for e in path:
+                    for y in e:
+                        del at[y][colour[e]]
+                for e in path:
+                    colour[e] = b if colour[e] == a else a
+                    for y in e:
+                        at[y][colour[e]] = e
+                c = a
+        else:
+            c = n_colours
+            n_colours += 1
+        colour[eid] = c
+        at[u][c] = eid
+        at[v][c] = eid
+    classes: List[List[EdgeID]] = [[] for _ in range(n_colours)]
+    for eid in graph.edges:
+        classes[colour[eid]].append(eid)
+    return [c for c in classes if c]

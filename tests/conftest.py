@@ -8,3 +8,4 @@ if ROOT not in sys.path:
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200) and the built libdqz.so")
+    config.addinivalue_line("markers", "slow: CPU test that takes more than ~20 s")

@@ -1,0 +1,157 @@
+"""GPU BPQuantumEmulator and BPEngine.
+
+* The reference's emulator test (quantum_emulator/test_bp_quantum_emulator.py:21-108)
+  on the GPU emulator, against the dense exact emulator: rho within the
+  reference's tolerances (3e-3 heavy cube, 1e-4 heavy hex / tree), identical
+  measurement outcomes for shared uniform samples.
+* The GPU emulator against the FP64 oracle emulator fed the same seeds:
+  same BP schedule (asynchronous DFS) and same random messages, so the
+  density matrices agree to 1e-9 and the truncation errors / entropies to 1e-9.
+* BPEngine sweeps (sync, async, flooding) against the oracle.
+"""
+
+import numpy as np
+import pytest
+import torch
+
+from dequantizer_b200 import BPQuantumEmulator
+from dequantizer_b200 import graph as G
+from dequantizer_b200.engine import BPEngine
+from dequantizer_b200.graph import MessageID, Node
+from oracle import maps as OM
+from oracle import tensor_ops as OT
+from oracle.emulator import BPQuantumEmulator as OracleEmulator
+from oracle.emulator import ExactQuantumEmulator
+from tests.helpers import heavy_cube, random_ising_q2_gate, random_q1_gate, random_tensors, rel_err, small_heavy_hex, to_np
+
+pytestmark = pytest.mark.gpu
+
+
+def _run(graph_factory, layers, accuracy, seed=42, compare_oracle=True):
+    rng = np.random.default_rng(seed)
+    g_gpu, g_exact, g_orc = graph_factory(), graph_factory(), graph_factory()
+    trav = list(g_gpu.get_traversal_iterator())
+    exact = ExactQuantumEmulator(g_exact)
+    gpu = BPQuantumEmulator(g_gpu, seed, 1024, g_gpu.edges_number, belief_propagation_accuracy=1e-6)
+    orc = OracleEmulator(g_orc, seed, 1024, g_orc.edges_number, belief_propagation_accuracy=1e-6) if compare_oracle else None
+    nodes = [el for el in trav if isinstance(el, Node)]
+    state = {n.id: int(rng.integers(0, 2)) for n in nodes}
+    exact.set_to_product_state(state)
+    gpu.set_to_product_state(state)
+    if orc:
+        orc.set_to_product_state(state)
+    for nid, s in state.items():
+        correct = np.zeros((2, 2))
+        correct[s, s] = 1.0
+        assert np.isclose(to_np(gpu.dens_q1(nid)), correct, atol=1e-8).all()
+        u = float(rng.uniform())
+        assert gpu.measure(nid, u) == s
+        if orc:
+            assert orc.measure(nid, u) == s
+    for _ in range(layers):
+        for el in trav:
+            if isinstance(el, Node):
+                g = random_q1_gate(rng)
+                for em in (exact, gpu, orc):
+                    if em is not None:
+                        em.apply_q1(g, el.id)
+            else:
+                g = random_ising_q2_gate(rng)
+                for em in (exact, gpu, orc):
+                    if em is not None:
+                        em.apply_q2(g, *el.id)
+    for el in nodes:
+        rho_g = to_np(gpu.dens_q1(el.id))
+        assert np.linalg.norm(exact.dens_q1(el.id) - rho_g) < accuracy
+        if orc:
+            assert np.abs(orc.dens_q1(el.id) - rho_g).max() < 1e-9
+    if orc:
+        te_g = np.array([float(x) for x in gpu.truncation_errors])
+        en_g = np.array([float(x) for x in gpu.entropies])
+        assert len(te_g) == len(orc.truncation_errors)
+        assert np.abs(te_g - np.array(orc.truncation_errors)).max() < 1e-9
+        assert np.abs(en_g - np.array(orc.entropies)).max() < 1e-9
+        assert gpu.bp_iterations == orc.bp_iterations
+    for el in nodes:
+        u = float(rng.uniform())
+        assert exact.measure(el.id, u) == gpu.measure(el.id, u)
+
+
+def test_gpu_emulator_heavy_cube():
+    _run(heavy_cube, 2, 3e-3)
+
+
+def test_gpu_emulator_small_heavy_hex():
+    _run(small_heavy_hex, 4, 1e-4)
+
+
+def test_gpu_emulator_random_tree():
+    _run(lambda: G.get_random_tree_tensor_graph(15, 2, 14 * [1], 42), 4, 1e-4)
+
+
+def test_emulator_regauges_per_reference_rule():
+    g = heavy_cube()
+    em = BPQuantumEmulator(g, 3, 8, 5, belief_propagation_accuracy=1e-6)
+    rng = np.random.default_rng(0)
+    edges = list(g.edges)
+    for i in range(12):
+        em.apply_q2(random_ising_q2_gate(rng), *edges[i])
+    # regauge before gates 6 and 11 -> two truncation-affected distances
+    assert len(em.truncated_affected_vidal_distances) == 2
+    assert len(em.truncation_errors) == 12
+    assert all(e.dimension <= 8 for e in g.edges.values())
+
+
+@pytest.mark.parametrize("schedule", ["sync", "async", "flooding"])
+def test_engine_sweeps_match_oracle(schedule):
+    g = G.get_random_regular_graph(16, 3, 2, 4, 5)
+    eng = BPEngine(g, traversal="dfs", schedule=schedule)
+    trav = eng.topo.traverser
+    tensors = random_tensors(g, 1)
+    rng = np.random.default_rng(2)
+    L = eng.layout
+    eng.load_tensors([tensors[n.id] for n in eng.topo.nodes])
+    mats = []
+    for h in range(L.n_halves):
+        z = rng.standard_normal((4, 4, 2))
+        a = z[..., 0] + 1j * z[..., 1]
+        mats.append(a @ a.conj().T)
+    e2n = []
+    for h in range(L.n_halves):
+        e2n.append(mats[int(L.half_twin[h])])
+    eng.load_messages(mats, e2n)
+    # oracle messages dict matching the packed state
+    msgs = {}
+    for h, (nd, e) in enumerate(eng.topo.half_ids()):
+        msgs[MessageID(nd.id, e.id)] = mats[h]
+        msgs[MessageID(e.id, nd.id)] = e2n[h]
+    if schedule == "flooding":
+        # node update reads the far end's previous node->edge message directly
+        def ref_sweep(t, m):
+            out = {}
+            for nd in eng.topo.nodes:
+                inc = [m[MessageID(e.neighbors[1].id if e.neighbors[0] is nd else e.neighbors[0].id, e.id)]
+                       for e in nd.neighbors]
+                new = OT.pass_through_node(t[nd.id], inc)
+                for e, x in zip(nd.neighbors, new):
+                    out[MessageID(nd.id, e.id)] = x
+            for nd in eng.topo.nodes:
+                for e in nd.neighbors:
+                    u = e.neighbors[1] if e.neighbors[0] is nd else e.neighbors[0]
+                    out[MessageID(e.id, nd.id)] = out[MessageID(u.id, e.id)]
+            return out
+    else:
+        ref_sweep = OM.get_belief_propagation_map(trav, schedule == "sync")
+    for _ in range(4):
+        msgs = ref_sweep(tensors, msgs)
+        eng.sweep()
+    for h, (nd, e) in enumerate(eng.topo.half_ids()):
+        assert rel_err(L.message_view(eng.n2e, h), msgs[MessageID(nd.id, e.id)]) < 1e-11
+        assert rel_err(L.message_view(eng.e2n, h), msgs[MessageID(e.id, nd.id)]) < 1e-11
+    iters = eng.run(1e-12, max_sweeps=300)
+    assert iters < 300
+    G_, lam = eng.vidal_gauge()
+    vd = float(eng.vidal_distance(G_, lam))
+    assert vd < 1e-8
+    rho = to_np(eng.densities())
+    assert np.allclose(np.trace(rho, axis1=1, axis2=2), 1.0)
