@@ -151,25 +151,6 @@ def barrier(world: int):
         dist.barrier()
 
 
-def measure_fp64_peak(torch):
-    """cuBLAS DGEMM throughput (best of 3, 8192^3), the FP64 roofline."""
-    n = 8192
-    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
-    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
-    torch.matmul(a, b)
-    torch.cuda.synchronize()
-    best = 1e30
-    for _ in range(3):
-        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        s.record()
-        torch.matmul(a, b)
-        e.record()
-        e.synchronize()
-        best = min(best, s.elapsed_time(e) * 1e-3)
-    del a, b
-    return 2.0 * n**3 / best / 1e12
-
-
 def cpu_baseline_sample(g, tensors_c64, m, seconds=12.0, threads=None):
     """Oracle pass_through_node over nodes (threads over nodes), on the host
     cores, for about ``seconds``; returns (edge-updates/s, threads, sample)."""
@@ -221,57 +202,65 @@ def run_reference(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
-def run_ours(args, world, rank, local):
+def measure_peak(torch, dtype):
+    """cuBLAS GEMM throughput (best of 3, 8192^3) for a real dtype: the FP64
+    (DGEMM) or FP32 (SGEMM, TF32 off) compute roofline of the node kernels."""
+    n = 8192
+    torch.backends.cuda.matmul.allow_tf32 = False
+    a = torch.randn(n, n, dtype=dtype, device="cuda")
+    b = torch.randn(n, n, dtype=dtype, device="cuda")
+    torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 1e30
+    for _ in range(3):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        torch.matmul(a, b)
+        e.record()
+        e.synchronize()
+        best = min(best, s.elapsed_time(e) * 1e-3)
+    del a, b
+    return 2.0 * n**3 / best / 1e12
+
+
+# DRAM bytes (read + write) per node-update launch from one ncu capture of
+# the bench workload; profiles/ holds the summaries these come from.
+NCU_TRAFFIC = {
+    ("bp_node_generic", "fp64"): 166.6e6,
+}
+
+
+def time_engine(args, world, g, packed_c64, m, precision, flush, clk=None):
+    """Device-timed sweeps and end-to-end sweeps for one precision."""
     import torch
 
     from dequantizer_b200.engine import BPEngine
 
-    g, tensors, m = workload(rank)
-    eng = BPEngine(g, traversal="dfs", schedule="sync")
+    eng = BPEngine(g, traversal="dfs", schedule="sync", precision=precision)
     L = eng.layout
-    # engine node order is the traversal order: permute once on the host
-    node_ids = list(g.nodes.keys())
-    pos = {nid: i for i, nid in enumerate(node_ids)}
-    perm = np.array([pos[n.id] for n in eng.topo.nodes])
-    packed_c64 = torch.from_numpy(np.ascontiguousarray(tensors[perm]).reshape(-1)).pin_memory()
-    n2e_host = torch.from_numpy(np.tile(m.reshape(-1), L.n_halves)).pin_memory()
+    mdt = torch.complex128 if precision == "fp64" else torch.complex64
+    n2e_host = torch.from_numpy(np.tile(m.reshape(-1), L.n_halves)).to(mdt).pin_memory()
     e2n_host = n2e_host.clone().pin_memory()
     out_host = torch.empty_like(n2e_host).pin_memory()
     eng.load_tensors_host(packed_c64)
     eng.load_messages_host(n2e_host, e2n_host)
     torch.cuda.synchronize()
-    edge_updates = L.n_halves
-    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     stream = torch.cuda.current_stream()
-
-    # warm-up
     for _ in range(args.warmup):
         eng.sweep()
     torch.cuda.synchronize()
-
-    # ---- device-timed sweeps (inputs resident, L2 flushed between steps)
     barrier(world)
-    torch.cuda.synchronize()
     times, node_times = [], []
-    with ClockSampler(local) as clk:
-        for _ in range(args.steps):
-            flush.zero_()
-            e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
-            e0.record(stream)
-            eng.sweep(mid_event=e1)
-            e2.record(stream)
-            e2.synchronize()
-            times.append(e0.elapsed_time(e2) * 1e-3)
-            node_times.append(e0.elapsed_time(e1) * 1e-3)
-    torch.cuda.synchronize()
+    for _ in range(args.steps):
+        flush.zero_()
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        e0.record(stream)
+        eng.sweep(mid_event=e1)
+        e2.record(stream)
+        e2.synchronize()
+        times.append(e0.elapsed_time(e2) * 1e-3)
+        node_times.append(e0.elapsed_time(e1) * 1e-3)
     barrier(world)
-    total = reduce_max(sum(times), world)
-    value = world * edge_updates * args.steps / total
-    node_avg = float(np.mean(node_times))
-
-    # ---- end to end: host buffers in, sweep, messages out
-    barrier(world)
-    torch.cuda.synchronize()
     e_times = []
     for _ in range(args.steps):
         flush.zero_()
@@ -284,41 +273,111 @@ def run_ours(args, world, rank, local):
         e.record(stream)
         e.synchronize()
         e_times.append(s.elapsed_time(e) * 1e-3)
+    eng.check()
+    edge_updates = L.n_halves
+    total = reduce_max(sum(times), world)
     e_total = reduce_max(sum(e_times), world)
-    e2e_value = world * edge_updates * args.steps / e_total
-    h2d = packed_c64.numel() * 8 + 2 * n2e_host.numel() * 16
-    d2h = out_host.numel() * 16
+    h2d = packed_c64.numel() * packed_c64.element_size() + 2 * n2e_host.numel() * n2e_host.element_size()
+    return {
+        "value": world * edge_updates * args.steps / total,
+        "ms_per_step": total / args.steps * 1e3,
+        "node_ms": float(np.mean(node_times)) * 1e3,
+        "e2e": world * edge_updates * args.steps / e_total,
+        "h2d": h2d,
+        "d2h": out_host.numel() * out_host.element_size(),
+        "launches": eng.launches_per_sweep() * args.steps,
+        "kernel": eng.kernel,
+        "edge_updates": edge_updates,
+    }
 
-    peak = measure_fp64_peak(torch) if rank == 0 else None
+
+def accuracy_check(g, packed_c64, m, tol=1e-6, max_sweeps=400):
+    """BP to convergence from the same start in fp64 and fp32; max |<Z_i>|
+    difference of the one-site density matrices (both read out in FP64)."""
+    import torch
+
+    from dequantizer_b200.engine import BPEngine
+
+    out = {}
+    for prec in ("fp64", "fp32"):
+        eng = BPEngine(g, traversal="dfs", schedule="sync", precision=prec)
+        mdt = torch.complex128 if prec == "fp64" else torch.complex64
+        msgs = torch.from_numpy(np.tile(m.reshape(-1), eng.layout.n_halves)).to(mdt)
+        eng.load_tensors_host(packed_c64)
+        eng.load_messages_host(msgs, msgs)
+        iters = eng.run(tol, max_sweeps=max_sweeps, check_every=5)
+        rho = eng.densities()
+        z = (rho[:, 0, 0] - rho[:, 1, 1]).real.double().cpu().numpy()
+        out[prec] = (z, iters, float(eng.distance()))
+    dz = float(np.abs(out["fp64"][0] - out["fp32"][0]).max())
+    return {"max_abs_dZ": dz, "bound": 1e-4, "ok": dz <= 1e-4, "tol": tol,
+            "sweeps_fp64": out["fp64"][1], "sweeps_fp32": out["fp32"][1],
+            "final_distance_fp64": out["fp64"][2], "final_distance_fp32": out["fp32"][2]}
+
+
+def run_ours(args, world, rank, local):
+    import torch
+
+    g, tensors, m = workload(rank)
+    from dequantizer_b200.maps import Topology
+
+    topo = Topology(list(g.get_traversal_iterator(ordering="dfs")), True)
+    pos = {nid: i for i, nid in enumerate(g.nodes.keys())}
+    perm = np.array([pos[n.id] for n in topo.nodes])
+    packed_c64 = torch.from_numpy(np.ascontiguousarray(tensors[perm]).reshape(-1)).pin_memory()
+    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    with ClockSampler(local) as clk:
+        r64 = time_engine(args, world, g, packed_c64, m, "fp64", flush) if args.only != "fp32" else None
+        r32 = time_engine(args, world, g, packed_c64, m, "fp32", flush) if args.only != "fp64" else None
+    if args.only:
+        r = r64 or r32
+        if rank == 0:
+            print(json.dumps({"only": args.only, "value": r["value"], "node_ms": r["node_ms"],
+                              "kernel": r["kernel"], "e2e": r["e2e"]}), flush=True)
+        return
+    acc = accuracy_check(g, packed_c64, m) if not args.no_accuracy else None
+    peak64 = measure_peak(torch, torch.float64) if rank == 0 else None
+    peak32 = measure_peak(torch, torch.float32) if rank == 0 else None
     if rank != 0:
         return
-    fl = flops_per_edge_update() * edge_updates
-    achieved = fl / node_avg / 1e12
-    traffic = None
-    tfile = os.path.join(ROOT, "profiles", "bp_node_generic_rr1024_chi16.traffic.json")
-    if os.path.exists(tfile):
-        with open(tfile) as f:
-            traffic = json.load(f).get("dram_bytes_per_launch")
+    fl = flops_per_edge_update() * r32["edge_updates"]
+
+    def roof(r, peak, prec):
+        ach = fl / (r["node_ms"] * 1e-3) / 1e12
+        return {"bound": "tensor", "achieved": ach, "peak": peak, "unit": "TFLOP/s",
+                "frac": ach / peak if peak else None,
+                "traffic": NCU_TRAFFIC.get((r["kernel"], prec)),
+                "kernel": r["kernel"],
+                "peak_source": ("cuBLAS DGEMM" if prec == "fp64" else "cuBLAS SGEMM (TF32 off)")
+                + " 8192^3 measured in this run (not in MEASURED_PEAKS.json)",
+                "flops_per_launch": fl, "launch_ms": r["node_ms"],
+                "algorithmic_bytes_per_launch": r["edge_updates"] * bytes_per_edge_update(
+                    s=16 if prec == "fp64" else 8)}
+
     cpu_v, cores, sample = (None, None, None)
     if world == 1 and not args.no_cpu:
         cpu_v, cores, sample = cpu_baseline_sample(g, tensors, m, seconds=args.cpu_seconds)
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": total / args.steps * 1e3, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+        "metric": METRIC, "value": r32["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": r32["ms_per_step"], "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "c64 (fp32)", "data": "synthetic",
         "config": {
             "workload": "random 3-regular graph (pairing model, seed 0), 1024 nodes, chi=16, d=2, complex64 "
-                        "inputs upcast to complex128: one synchronous BP sweep = 3072 edge-updates per step",
-            "precision": "fp64 (complex128)", "schedule": "reference synchronous sweep",
+                        "node tensors: one synchronous BP sweep = 3072 edge-updates per step",
+            "precision": "fp32 sweeps (complex64); gauge / distance / densities in fp64",
+            "schedule": "reference synchronous sweep",
             "l2": "flushed between steps (512 MB write)", "parallelism": f"replicas x{world}",
         },
-        "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                     "frac": achieved / peak if peak else None, "traffic": traffic,
-                     "kernel": "bp_node_generic", "peak_source": "cuBLAS DGEMM 8192^3 measured in this run",
-                     "flops_per_launch": fl, "launch_ms": node_avg * 1e3},
+        "fp64": {"value": r64["value"], "ms_per_step": r64["ms_per_step"], "e2e": r64["e2e"],
+                 "roofline": roof(r64, peak64, "fp64")},
+        "speedup_vs_fp64": r32["value"] / r64["value"],
+        "accuracy": acc,
+        "roofline": roof(r32, peak32, "fp32"),
         "cpu_baseline": {"value": cpu_v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
-        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-        "gpu_launches": eng.launches_per_sweep() * args.steps,
+        "e2e": {"value": r32["e2e"], "unit": UNIT, "h2d_bytes_per_step": r32["h2d"],
+                "d2h_bytes_per_step": r32["d2h"]},
+        "gpu_launches": r32["launches"],
         "clocks": clk.summary(),
     }
     print(json.dumps(line), flush=True)
@@ -333,6 +392,9 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--ref-seconds", type=float, default=8.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-accuracy", action="store_true")
+    ap.add_argument("--only", choices=["fp64", "fp32"], default=None,
+                    help="time one precision only (profiling runs); prints a short line")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

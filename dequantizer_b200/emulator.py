@@ -67,8 +67,12 @@ class BPQuantumEmulator:
         self._node_idx = {n.id: i for i, n in enumerate(self._nodes)}
         self._passed = 0
         self._pending: List[tuple] = []
+        # per-gate truncation errors / entropies, in chunks per executed level
+        # with the gates' application order numbers
         self._err_chunks: List[torch.Tensor] = []
         self._ent_chunks: List[torch.Tensor] = []
+        self._seq_chunks: List[torch.Tensor] = []
+        self._q2_count = 0
         self._after_vd: List[torch.Tensor] = []
         self._trunc_vd: List[torch.Tensor] = []
         self.bp_iterations: List[int] = []
@@ -132,12 +136,18 @@ class BPQuantumEmulator:
     @property
     def truncation_errors(self) -> List[torch.Tensor]:
         self._flush()
-        return list(torch.cat(self._err_chunks)) if self._err_chunks else []
+        return list(self._ordered(self._err_chunks))
 
     @property
     def entropies(self) -> List[torch.Tensor]:
         self._flush()
-        return list(torch.cat(self._ent_chunks)) if self._ent_chunks else []
+        return list(self._ordered(self._ent_chunks))
+
+    def _ordered(self, chunks) -> torch.Tensor:
+        if not chunks:
+            return torch.zeros(0, dtype=torch.float64)
+        seq = torch.cat(self._seq_chunks)
+        return torch.cat(chunks)[torch.argsort(seq)]
 
     def set_to_product_state(self, state: Dict):
         """bp_quantum_emulator.py:110-130."""
@@ -227,7 +237,8 @@ class BPQuantumEmulator:
         self._grow({v1: s1, v2: s2}, {e: new_chi})
         L = self._layout
         first = 1 if edge.neighbors[0] is n1 else 0
-        self._pending.append(("q2", v1, v2, e, first, halves, rank, max(m1, m2), k))
+        self._pending.append(("q2", v1, v2, e, first, halves, rank, max(m1, m2), k, self._q2_count))
+        self._q2_count += 1
         # host bookkeeping, as tensor_graph.py:366-374
         L.edge_chi[e] = new_chi
         edge.dimension = new_chi
@@ -280,6 +291,7 @@ class BPQuantumEmulator:
                           err.data_ptr(), ent.data_ptr(), scratch.data_ptr(), stream)
                 self._err_chunks.append(err)
                 self._ent_chunks.append(ent)
+                self._seq_chunks.append(torch.tensor([op[9] for op in q2], dtype=torch.int64, device=dev))
         self._rho_cache = None
 
     # ---------------------------------------------------------- regauge

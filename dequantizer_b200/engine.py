@@ -11,10 +11,14 @@ and exposes whole-graph operations on them:
   message sets (mappings/messages_distance.py:14-22);
 * ``run()``              -- sweeps to a tolerance, like the reference's
   driver loops (examples/3d_ising_canonicalization.py:137-145);
-* ``vidal_gauge()`` / ``vidal_distance()`` / ``densities()``.
+* ``vidal_gauge()`` / ``vidal_distance()`` / ``densities()`` (FP64).
 
-Host arrays can be loaded and read back through pinned staging buffers
-(``load_tensors_host`` / ``read_messages_host``), the end-to-end path.
+``precision="fp64"`` keeps complex128 arenas (the plain form);
+``precision="fp32"`` keeps complex64 arenas and runs the sweeps in FP32
+(degree-3 nodes with bonds of dimension 8 or 16), while the gauge,
+distance and density computations are still done in FP64 on upcast copies.
+Host arrays are loaded and read back through the ``*_host`` methods, the
+end-to-end path.
 """
 
 from typing import List, Optional, Sequence
@@ -25,35 +29,46 @@ import torch
 from . import _lib
 from .graph import TensorGraph
 from .layout import GraphLayout
-from .maps import Topology, bp_sweep, density_packed, vidal_distance_packed, vidal_gauge_packed
+from .maps import Topology, bp_sweep, density_packed, error_flag, vidal_distance_packed, vidal_gauge_packed
 
 SCHEDULES = ("sync", "async", "flooding")
+PRECISIONS = {"fp64": torch.complex128, "fp32": torch.complex64}
 
 
 class BPEngine:
-    def __init__(self, graph: TensorGraph, traversal: str = "dfs", schedule: str = "sync", device=None):
+    def __init__(self, graph: TensorGraph, traversal: str = "dfs", schedule: str = "sync", precision: str = "fp64",
+                 device=None):
         if schedule not in SCHEDULES:
             raise ValueError(f"schedule must be one of {SCHEDULES}")
+        if precision not in PRECISIONS:
+            raise ValueError(f"precision must be one of {tuple(PRECISIONS)}")
         if not torch.cuda.is_available():
             raise RuntimeError("BPEngine runs on the GPU only and no CUDA device is available")
         _lib.lib()
         self.graph = graph
+        self.precision = precision
+        self.dtype = PRECISIONS[precision]
         trav = list(graph.get_traversal_iterator(ordering=traversal))
         self.topo = Topology(trav, schedule == "sync", flooding=schedule == "flooding")
         chi = [e.dimension for e in self.topo.edges]
         self.layout = GraphLayout(self.topo.nodes, self.topo.edges, chi, device=device)
         L = self.layout
-        self.T = L.new_tensor_arena()
-        self.n2e = L.new_msg_arena()
-        self.e2n = L.new_msg_arena()
-        self._n2e_prev: Optional[torch.Tensor] = None
-        self._e2n_prev: Optional[torch.Tensor] = None
-        self._spare = (L.new_msg_arena(), L.new_msg_arena())
+        if precision == "fp32" and not L.uniform_k3_chi():
+            raise NotImplementedError("fp32 sweeps need degree-3 nodes with bonds of dimension 8 or 16")
+        self.T = self._arena(L.tensor_elems)
+        self.n2e = self._arena(L.msg_elems)
+        self.e2n = self._arena(L.msg_elems)
+        self._prev = None
+        self._spare = (self._arena(L.msg_elems), self._arena(L.msg_elems))
         self._partial = torch.empty(max(2 * L.n_halves, 1), dtype=torch.float64, device=L.device)
-        nb = _lib.lib().dqz_bp_node_scratch_bytes(max(len(l) for l in self.topo.levels), L.max_slice(),
-                                                 L.max_chi())
-        self._scratch = torch.empty(nb, dtype=torch.uint8, device=L.device) if nb else None
-        self._pinned = {}
+        self._stage = {}
+
+    def _arena(self, n):
+        return torch.zeros(max(n, 1), dtype=self.dtype, device=self.layout.device)
+
+    @property
+    def kernel(self) -> str:
+        return "bp_node_k3" if self.layout.uniform_k3_chi() else "bp_node_generic"
 
     # -------------------------------------------------------------- load
     def load_tensors(self, tensors_by_node: Sequence) -> None:
@@ -62,43 +77,37 @@ class BPEngine:
         for v, t in enumerate(tensors_by_node):
             tt = t if isinstance(t, torch.Tensor) else torch.from_numpy(np.asarray(t))
             o = int(L.node_off[v])
-            self.T[o : o + tt.numel()] = tt.reshape(-1).to(L.device, torch.complex128)
+            self.T[o : o + tt.numel()] = tt.reshape(-1).to(L.device, self.dtype)
 
     def load_messages(self, n2e_by_half: Sequence, e2n_by_half: Optional[Sequence] = None) -> None:
         L = self.layout
-        for arena, mats in ((self.n2e, n2e_by_half), (self.e2n, e2n_by_half if e2n_by_half is not None else n2e_by_half)):
+        e2n_by_half = e2n_by_half if e2n_by_half is not None else n2e_by_half
+        for arena, mats in ((self.n2e, n2e_by_half), (self.e2n, e2n_by_half)):
             for h, m in enumerate(mats):
                 mm = m if isinstance(m, torch.Tensor) else torch.from_numpy(np.asarray(m))
                 o = int(L.half_msg_off[h])
-                arena[o : o + mm.numel()] = mm.reshape(-1).to(L.device, torch.complex128)
+                arena[o : o + mm.numel()] = mm.reshape(-1).to(L.device, self.dtype)
 
-    def _pin(self, name, numel, dtype):
-        buf = self._pinned.get(name)
-        if buf is None or buf.numel() != numel or buf.dtype != dtype:
-            buf = torch.empty(numel, dtype=dtype, pin_memory=True)
-            self._pinned[name] = buf
-        return buf
+    def _staged(self, src: torch.Tensor, dst: torch.Tensor) -> None:
+        """Asynchronous H2D of a pinned host arena into ``dst``; a dtype
+        change happens on the device after the copy."""
+        if src.dtype == dst.dtype:
+            dst.copy_(src, non_blocking=True)
+            return
+        key = (src.numel(), src.dtype)
+        buf = self._stage.get(key)
+        if buf is None:
+            buf = torch.empty(src.numel(), dtype=src.dtype, device=self.layout.device)
+            self._stage[key] = buf
+        buf.copy_(src, non_blocking=True)
+        dst.copy_(buf)
 
     def load_tensors_host(self, packed: torch.Tensor) -> None:
-        """Asynchronous H2D of a packed host arena (complex64 or complex128,
-        pinned) into the tensor arena, converted on the device."""
-        if packed.dtype == torch.complex128:
-            self.T.copy_(packed, non_blocking=True)
-        else:
-            stage = self._stage("t_stage", packed.numel(), packed.dtype)
-            stage.copy_(packed, non_blocking=True)
-            self.T.copy_(stage)
-
-    def _stage(self, name, numel, dtype):
-        buf = self._pinned.get("dev_" + name)
-        if buf is None or buf.numel() != numel or buf.dtype != dtype:
-            buf = torch.empty(numel, dtype=dtype, device=self.layout.device)
-            self._pinned["dev_" + name] = buf
-        return buf
+        self._staged(packed, self.T)
 
     def load_messages_host(self, n2e: torch.Tensor, e2n: torch.Tensor) -> None:
-        self.n2e.copy_(n2e, non_blocking=True)
-        self.e2n.copy_(e2n, non_blocking=True)
+        self._staged(n2e, self.n2e)
+        self._staged(e2n, self.e2n)
 
     def read_messages_host(self, out_n2e: torch.Tensor) -> None:
         out_n2e.copy_(self.n2e, non_blocking=True)
@@ -109,34 +118,33 @@ class BPEngine:
         ``mid_event`` (a torch.cuda.Event) is recorded between the node
         updates and the edge pass, to time the node-update kernel alone."""
         n2e_new, e2n_new = self._spare
-        L = self.layout
-        src_sel, edge_new, levels = self.topo.device_tables(L.device)
-        stream = _lib.stream_handle()
-        ms, mc = L.max_slice(), L.max_chi()
-        for halves in levels:
-            _lib.call("dqz_bp_node_update", L.gptr, self.T.data_ptr(), self.n2e.data_ptr(), self.e2n.data_ptr(),
-                      n2e_new.data_ptr(), src_sel.data_ptr(), halves.data_ptr(), halves.numel(), ms, mc,
-                      _lib.ptr(self._scratch), stream)
-        if mid_event is not None:
-            mid_event.record(torch.cuda.current_stream())
-        _lib.call("dqz_bp_edge_pass", L.gptr, self.n2e.data_ptr(), n2e_new.data_ptr(), edge_new.data_ptr(),
-                  e2n_new.data_ptr(), mc, stream)
+        bp_sweep(self.layout, self.topo, self.T, self.n2e, self.e2n, n2e_new, e2n_new, mid_event)
         self._spare = (self.n2e, self.e2n)
-        self._n2e_prev, self._e2n_prev = self.n2e, self.e2n
+        self._prev = (self.n2e, self.e2n)
         self.n2e, self.e2n = n2e_new, e2n_new
 
     def launches_per_sweep(self) -> int:
         return len(self.topo.levels) + 1
 
+    def check(self) -> None:
+        """Raises when a kernel skipped a node of an unexpected shape."""
+        if int(error_flag(self.layout.device).item()):
+            raise RuntimeError("a BP kernel met a node outside its supported shape")
+
+    def _c128(self, x: torch.Tensor) -> torch.Tensor:
+        return x if x.dtype == torch.complex128 else x.to(torch.complex128)
+
     def distance(self) -> torch.Tensor:
-        """Mean Frobenius distance between the current and previous messages."""
-        if self._n2e_prev is None:
+        """Mean Frobenius distance between the current and previous messages (FP64)."""
+        if self._prev is None:
             raise RuntimeError("distance() needs at least one sweep")
         L = self.layout
         out = torch.empty((), dtype=torch.float64, device=L.device)
-        _lib.call("dqz_messages_distance", L.gptr, self.n2e.data_ptr(), self._n2e_prev.data_ptr(),
-                  self.e2n.data_ptr(), self._e2n_prev.data_ptr(), self._partial.data_ptr(), out.data_ptr(),
-                  L.max_chi(), _lib.stream_handle())
+        # keep the (possibly converted) operands alive across the call: a
+        # temporary's memory could be handed to the next conversion otherwise
+        ops = [self._c128(x) for x in (self.n2e, self._prev[0], self.e2n, self._prev[1])]
+        _lib.call("dqz_messages_distance", L.gptr, *(x.data_ptr() for x in ops), self._partial.data_ptr(),
+                  out.data_ptr(), L.max_chi(), _lib.stream_handle())
         return out
 
     def run(self, tol: float, max_sweeps: int = 1000, check_every: int = 1) -> int:
@@ -148,14 +156,14 @@ class BPEngine:
         return max_sweeps
 
     def vidal_gauge(self, eps: float = 1e-10):
-        return vidal_gauge_packed(self.layout, self.T, self.n2e, eps)
+        return vidal_gauge_packed(self.layout, self._c128(self.T), self._c128(self.n2e), eps)
 
     def vidal_distance(self, G, lam, eps: float = 1e-10) -> torch.Tensor:
         return vidal_distance_packed(self.layout, G, lam, eps)
 
     def densities(self, nodes: Optional[List[int]] = None) -> torch.Tensor:
         nodes = list(range(self.layout.n_nodes)) if nodes is None else nodes
-        return density_packed(self.layout, self.T, self.e2n, nodes)
+        return density_packed(self.layout, self._c128(self.T), self._c128(self.e2n), nodes)
 
     def messages(self) -> List[torch.Tensor]:
         return [self.layout.message_view(self.n2e, h) for h in range(self.layout.n_halves)]

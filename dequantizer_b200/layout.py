@@ -105,6 +105,19 @@ class GraphLayout:
     def half_chi(self) -> np.ndarray:
         return self.edge_chi[self.half_edge]
 
+    def uniform_k3_chi(self) -> int:
+        """Bond dimension when every node has degree 3 and physical dimension
+        2 and every edge the same bond dimension in {8, 16} (the shapes the
+        specialised node-update kernel covers); 0 otherwise."""
+        if not self.n_nodes or not self.n_edges:
+            return 0
+        if not (np.all(self.degree == 3) and np.all(self.phys == 2)):
+            return 0
+        chi = int(self.edge_chi[0])
+        if chi not in (8, 16) or not np.all(self.edge_chi == chi) or np.any(self.half_edge < 0):
+            return 0
+        return chi
+
     # ------------------------------------------------------------ offsets
     def _finish(self):
         self.node_off = np.zeros(self.n_nodes, dtype=np.int64)

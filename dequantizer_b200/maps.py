@@ -153,10 +153,51 @@ class _LayoutCache:
         return self._layout
 
 
-def bp_sweep(layout: GraphLayout, topo: Topology, T, n2e_old, e2n_old, n2e_new, e2n_new):
-    """One sweep on packed arenas: node updates level by level, then the edge pass."""
+_ERROR_FLAGS = {}
+
+
+def error_flag(device) -> torch.Tensor:
+    """Device int set by kernels that skip work items of an unexpected shape."""
+    key = str(device)
+    if key not in _ERROR_FLAGS:
+        _ERROR_FLAGS[key] = torch.zeros(1, dtype=torch.int32, device=device)
+    return _ERROR_FLAGS[key]
+
+
+def bp_sweep(layout: GraphLayout, topo: Topology, T, n2e_old, e2n_old, n2e_new, e2n_new, mid_event=None):
+    """One sweep on packed arenas: node updates level by level, then the edge pass
+    (``mid_event``, a torch.cuda.Event, is recorded between the two).
+
+    complex128 arenas use the specialised degree-3 kernel when every node
+    has that shape (layout.uniform_k3_chi), the generic kernel otherwise;
+    complex64 arenas need the specialised shape."""
     src_sel, edge_new, levels = topo.device_tables(layout.device)
     stream = _lib.stream_handle()
+    chi3 = layout.uniform_k3_chi()
+    if T.dtype == torch.complex64:
+        if not chi3:
+            raise NotImplementedError("complex64 BP needs degree-3 nodes with bonds of dimension 8 or 16")
+        flag = error_flag(layout.device)
+        for halves in levels:
+            _lib.call("dqz_bp_node_update_k3", layout.gptr, chi3, 32, T.data_ptr(), n2e_old.data_ptr(),
+                      e2n_old.data_ptr(), n2e_new.data_ptr(), src_sel.data_ptr(), halves.data_ptr(), halves.numel(),
+                      flag.data_ptr(), stream)
+        if mid_event is not None:
+            mid_event.record(torch.cuda.current_stream())
+        _lib.call("dqz_bp_edge_pass_c64", layout.gptr, n2e_old.data_ptr(), n2e_new.data_ptr(), edge_new.data_ptr(),
+                  e2n_new.data_ptr(), stream)
+        return
+    if chi3:
+        flag = error_flag(layout.device)
+        for halves in levels:
+            _lib.call("dqz_bp_node_update_k3", layout.gptr, chi3, 64, T.data_ptr(), n2e_old.data_ptr(),
+                      e2n_old.data_ptr(), n2e_new.data_ptr(), src_sel.data_ptr(), halves.data_ptr(), halves.numel(),
+                      flag.data_ptr(), stream)
+        if mid_event is not None:
+            mid_event.record(torch.cuda.current_stream())
+        _lib.call("dqz_bp_edge_pass", layout.gptr, n2e_old.data_ptr(), n2e_new.data_ptr(), edge_new.data_ptr(),
+                  e2n_new.data_ptr(), chi3, stream)
+        return
     max_slice, max_chi = layout.max_slice(), layout.max_chi()
     scratch = None
     nbytes = _lib.lib().dqz_bp_node_scratch_bytes(max(len(l) for l in topo.levels), max_slice, max_chi)
@@ -168,6 +209,8 @@ def bp_sweep(layout: GraphLayout, topo: Topology, T, n2e_old, e2n_old, n2e_new, 
             n2e_new.data_ptr(), src_sel.data_ptr(), halves.data_ptr(), halves.numel(), max_slice, max_chi,
             _lib.ptr(scratch), stream,
         )
+    if mid_event is not None:
+        mid_event.record(torch.cuda.current_stream())
     _lib.call(
         "dqz_bp_edge_pass", layout.gptr, n2e_old.data_ptr(), n2e_new.data_ptr(), edge_new.data_ptr(),
         e2n_new.data_ptr(), max_chi, stream,

@@ -87,6 +87,21 @@ int dqz_bp_node_update(const dqz_graph_t *g, const void *tensors /*c128*/,
                        int32_t max_slice, int32_t max_chi, void *scratch, cudaStream_t stream);
 size_t dqz_bp_node_scratch_bytes(int32_t n_halves, int32_t max_slice, int32_t max_chi);
 
+/* Node update specialised for degree-3 nodes whose three bonds all have
+ * dimension `chi` (8 or 16) and physical dimension 2, e.g. random 3-regular
+ * graphs. Same result as dqz_bp_node_update (tensor_ops.py:36-60).
+ * precision 64: tensors and messages complex128; precision 32: complex64
+ * with FP32 arithmetic. A node of any other shape is skipped and sets
+ * *error_flag (device int) to 1. Needs no scratch. */
+int dqz_bp_node_update_k3(const dqz_graph_t *g, int32_t chi, int32_t precision, const void *tensors,
+                          const void *n2e_old, const void *e2n_old, void *n2e_new,
+                          const uint8_t *src_sel, const int32_t *halves, int32_t n_halves,
+                          int32_t *error_flag, cudaStream_t stream);
+
+/* Edge pass on complex64 messages (see dqz_bp_edge_pass). */
+int dqz_bp_edge_pass_c64(const dqz_graph_t *g, const void *n2e_old, const void *n2e_new,
+                         const uint8_t *edge_new, void *e2n_new, cudaStream_t stream);
+
 /* Edge pass (tensor_ops.py:70-76): e2n_new[h] = (edge_new[h] ? n2e_new : n2e_old)[twin(h)]
  * for every half-edge. */
 int dqz_bp_edge_pass(const dqz_graph_t *g, const void *n2e_old, const void *n2e_new,

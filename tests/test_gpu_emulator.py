@@ -102,6 +102,34 @@ def test_emulator_regauges_per_reference_rule():
     assert all(e.dimension <= 8 for e in g.edges.values())
 
 
+@pytest.mark.parametrize("chi", [8, 16])
+def test_engine_fp32_sweeps_track_fp64(chi):
+    """complex64 sweeps (FP32 arithmetic) stay within FP32 rounding of the
+    complex128 sweeps from the same start; tolerance 1e-5 relative."""
+    g = G.get_random_regular_graph(32, 3, 2, chi, 9)
+    tensors = random_tensors(g, 5)
+    e64 = BPEngine(g, schedule="sync", precision="fp64")
+    e32 = BPEngine(g, schedule="sync", precision="fp32")
+    order = [tensors[n.id] / np.linalg.norm(tensors[n.id]) for n in e64.topo.nodes]
+    rng = np.random.default_rng(6)
+    mats = []
+    for h in range(e64.layout.n_halves):
+        z = rng.standard_normal((chi, chi, 2))
+        a = z[..., 0] + 1j * z[..., 1]
+        m = a @ a.conj().T
+        mats.append(m / np.trace(m).real)
+    for e in (e64, e32):
+        e.load_tensors(order)
+        e.load_messages(mats)
+    for _ in range(5):
+        e64.sweep()
+        e32.sweep()
+    a = e64.n2e
+    b = e32.n2e.to(torch.complex128)
+    assert float((a - b).abs().max() / a.abs().max()) < 1e-5
+    e32.check()
+
+
 @pytest.mark.parametrize("schedule", ["sync", "async", "flooding"])
 def test_engine_sweeps_match_oracle(schedule):
     g = G.get_random_regular_graph(16, 3, 2, 4, 5)

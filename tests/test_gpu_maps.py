@@ -56,6 +56,25 @@ def test_bp_sweep_matches_oracle(case, ordering, sync):
     assert abs(d_ref - d_gpu) < 1e-10 * max(1.0, d_ref)
 
 
+@pytest.mark.parametrize("sync", [True, False])
+@pytest.mark.parametrize("chi", [8, 16])
+def test_degree3_kernel_matches_oracle(chi, sync):
+    """Uniform degree-3 graphs take the specialised kernel (bp_node_k3)."""
+    g = G.get_random_regular_graph(10, 3, 2, chi, 7)
+    trav = list(g.get_traversal_iterator(ordering="dfs"))
+    tensors = random_tensors(g, 3)
+    messages = random_messages(g, 4)
+    ref = OM.get_belief_propagation_map(trav, sync)
+    gpu = M.get_belief_propagation_map(trav, sync)
+    r_msgs, g_msgs = messages, messages
+    for _ in range(3):
+        r_msgs = ref(tensors, r_msgs)
+        g_msgs = gpu(tensors, g_msgs)
+    for k in r_msgs:
+        assert rel_err(g_msgs[k], r_msgs[k]) < TOL, k
+    assert int(M.error_flag(torch.device("cuda", 0)).item()) == 0
+
+
 def _converged_messages(g, tensors, n=200, tol=1e-13):
     trav = list(g.get_traversal_iterator())
     bp = OM.get_belief_propagation_map(trav)
