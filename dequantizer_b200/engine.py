@@ -32,7 +32,7 @@ from .layout import GraphLayout
 from .maps import Topology, bp_sweep, density_packed, error_flag, vidal_distance_packed, vidal_gauge_packed
 
 SCHEDULES = ("sync", "async", "flooding")
-PRECISIONS = {"fp64": torch.complex128, "fp32": torch.complex64}
+PRECISIONS = {"fp64": torch.complex128, "fp32": torch.complex64, "bf16": torch.complex64}
 
 
 class BPEngine:
@@ -55,6 +55,8 @@ class BPEngine:
         L = self.layout
         if precision == "fp32" and not L.uniform_k3_chi():
             raise NotImplementedError("fp32 sweeps need degree-3 nodes with bonds of dimension 8 or 16")
+        if precision == "bf16" and L.uniform_k3_chi() != 16:
+            raise NotImplementedError("bf16 tensor-core sweeps need degree-3 nodes with bonds of dimension 16")
         self.T = self._arena(L.tensor_elems)
         self.n2e = self._arena(L.msg_elems)
         self.e2n = self._arena(L.msg_elems)
@@ -68,6 +70,8 @@ class BPEngine:
 
     @property
     def kernel(self) -> str:
+        if self.precision == "bf16":
+            return "bp_node_k3_bf16"
         return "bp_node_k3" if self.layout.uniform_k3_chi() else "bp_node_generic"
 
     # -------------------------------------------------------------- load
@@ -118,7 +122,8 @@ class BPEngine:
         ``mid_event`` (a torch.cuda.Event) is recorded between the node
         updates and the edge pass, to time the node-update kernel alone."""
         n2e_new, e2n_new = self._spare
-        bp_sweep(self.layout, self.topo, self.T, self.n2e, self.e2n, n2e_new, e2n_new, mid_event)
+        bp_sweep(self.layout, self.topo, self.T, self.n2e, self.e2n, n2e_new, e2n_new, mid_event,
+                 tensor_cores=self.precision == "bf16")
         self._spare = (self.n2e, self.e2n)
         self._prev = (self.n2e, self.e2n)
         self.n2e, self.e2n = n2e_new, e2n_new

@@ -164,22 +164,27 @@ def error_flag(device) -> torch.Tensor:
     return _ERROR_FLAGS[key]
 
 
-def bp_sweep(layout: GraphLayout, topo: Topology, T, n2e_old, e2n_old, n2e_new, e2n_new, mid_event=None):
+def bp_sweep(layout: GraphLayout, topo: Topology, T, n2e_old, e2n_old, n2e_new, e2n_new, mid_event=None,
+             tensor_cores: bool = False):
     """One sweep on packed arenas: node updates level by level, then the edge pass
     (``mid_event``, a torch.cuda.Event, is recorded between the two).
 
     complex128 arenas use the specialised degree-3 kernel when every node
     has that shape (layout.uniform_k3_chi), the generic kernel otherwise;
-    complex64 arenas need the specialised shape."""
+    complex64 arenas need the specialised shape and run in FP32, or with
+    ``tensor_cores`` as BF16 tensor-core products with FP32 accumulation
+    (bonds of dimension 16)."""
     src_sel, edge_new, levels = topo.device_tables(layout.device)
     stream = _lib.stream_handle()
     chi3 = layout.uniform_k3_chi()
     if T.dtype == torch.complex64:
-        if not chi3:
-            raise NotImplementedError("complex64 BP needs degree-3 nodes with bonds of dimension 8 or 16")
+        if not chi3 or (tensor_cores and chi3 != 16):
+            raise NotImplementedError("complex64 BP needs degree-3 nodes with bonds of dimension 8 or 16 "
+                                      "(16 for the tensor-core form)")
         flag = error_flag(layout.device)
+        code = 16 if tensor_cores else 32
         for halves in levels:
-            _lib.call("dqz_bp_node_update_k3", layout.gptr, chi3, 32, T.data_ptr(), n2e_old.data_ptr(),
+            _lib.call("dqz_bp_node_update_k3", layout.gptr, chi3, code, T.data_ptr(), n2e_old.data_ptr(),
                       e2n_old.data_ptr(), n2e_new.data_ptr(), src_sel.data_ptr(), halves.data_ptr(), halves.numel(),
                       flag.data_ptr(), stream)
         if mid_event is not None:

@@ -130,6 +130,53 @@ def test_engine_fp32_sweeps_track_fp64(chi):
     e32.check()
 
 
+def _bench_like(n, seed, chi=16):
+    g = G.get_random_regular_graph(n, 3, 2, chi, seed)
+    rng = np.random.default_rng(seed + 100)
+    tensors = []
+    for _ in range(n):
+        z = rng.standard_normal((chi**3 * 2, 2))
+        tensors.append((z[:, 0] + 1j * z[:, 1]) / np.sqrt(2 * 2 * chi**3))
+    a = rng.standard_normal((chi, chi, 2))
+    a = a[..., 0] + 1j * a[..., 1]
+    m = a @ a.conj().T
+    return g, tensors, m / np.trace(m).real
+
+
+def test_engine_bf16_sweeps_track_fp64():
+    """BF16 tensor-core sweeps from the same start stay within BF16 operand
+    rounding (relative 3e-2 per message entry) of the FP64 sweeps."""
+    g, tensors, m = _bench_like(48, 3)
+    engines = {p: BPEngine(g, schedule="sync", precision=p) for p in ("fp64", "bf16")}
+    for e in engines.values():
+        e.load_tensors(tensors)
+        e.load_messages([m] * e.layout.n_halves)
+    for _ in range(4):
+        for e in engines.values():
+            e.sweep()
+    a = engines["fp64"].n2e
+    b = engines["bf16"].n2e.to(torch.complex128)
+    assert float((a - b).abs().max() / a.abs().max()) < 3e-2
+    engines["bf16"].check()
+
+
+def test_engine_bf16_meets_z_bound_at_fixed_point():
+    """<Z_i> after BP to the fixed point: BF16 sweeps vs FP64 sweeps,
+    |delta <Z_i>| <= 1e-4 (the mixed-precision accuracy bound)."""
+    g, tensors, m = _bench_like(96, 5)
+    z = {}
+    for p in ("fp64", "bf16", "fp32"):
+        e = BPEngine(g, schedule="sync", precision=p)
+        e.load_tensors(tensors)
+        e.load_messages([m] * e.layout.n_halves)
+        for _ in range(80):
+            e.sweep()
+        rho = to_np(e.densities())
+        z[p] = (rho[:, 0, 0] - rho[:, 1, 1]).real
+    assert np.abs(z["fp32"] - z["fp64"]).max() < 1e-6
+    assert np.abs(z["bf16"] - z["fp64"]).max() < 1e-4
+
+
 @pytest.mark.parametrize("schedule", ["sync", "async", "flooding"])
 def test_engine_sweeps_match_oracle(schedule):
     g = G.get_random_regular_graph(16, 3, 2, 4, 5)
