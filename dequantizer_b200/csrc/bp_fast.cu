@@ -286,10 +286,6 @@ __global__ void edge_pass_words(dqz_graph_t g, const W *n2e_old, const W *n2e_ne
 
 }  // namespace
 
-int dqz_launch_k3_bf16(const dqz_graph_t *g, const void *T, const void *n2e_old, const void *e2n_old, void *n2e_new,
-                       const uint8_t *src_sel, const int32_t *halves, int n_halves, int *error_flag,
-                       cudaStream_t stream);
-
 extern "C" int dqz_bp_node_update_k3(const dqz_graph_t *g, int32_t chi, int32_t precision, const void *tensors,
                                      const void *n2e_old, const void *e2n_old, void *n2e_new, const uint8_t *src_sel,
                                      const int32_t *halves, int32_t n_halves, int32_t *error_flag,
@@ -302,9 +298,6 @@ extern "C" int dqz_bp_node_update_k3(const dqz_graph_t *g, int32_t chi, int32_t 
                                                  error_flag, stream);
     if (chi == 8) return launch_k3<8, double2>(g, tensors, n2e_old, e2n_old, n2e_new, src_sel, halves, n_halves,
                                                error_flag, stream);
-  } else if (precision == 16) {
-    if (chi == 16)
-      return dqz_launch_k3_bf16(g, tensors, n2e_old, e2n_old, n2e_new, src_sel, halves, n_halves, error_flag, stream);
   } else if (precision == 32) {
     if (chi == 16) return launch_k3<16, float2>(g, tensors, n2e_old, e2n_old, n2e_new, src_sel, halves, n_halves,
                                                 error_flag, stream);

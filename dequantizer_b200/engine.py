@@ -64,6 +64,11 @@ class BPEngine:
         self._spare = (self._arena(L.msg_elems), self._arena(L.msg_elems))
         self._partial = torch.empty(max(2 * L.n_halves, 1), dtype=torch.float64, device=L.device)
         self._stage = {}
+        # bf16: node tensors also kept as BF16 planes (16384 per node), rebuilt
+        # from T after every load
+        self.T_bf16 = (torch.empty(L.n_nodes * 16384, dtype=torch.bfloat16, device=L.device)
+                       if precision == "bf16" else None)
+        self._bf16_stale = True
 
     def _arena(self, n):
         return torch.zeros(max(n, 1), dtype=self.dtype, device=self.layout.device)
@@ -71,7 +76,7 @@ class BPEngine:
     @property
     def kernel(self) -> str:
         if self.precision == "bf16":
-            return "bp_node_k3_bf16"
+            return "bp_node_k3_tc"
         return "bp_node_k3" if self.layout.uniform_k3_chi() else "bp_node_generic"
 
     # -------------------------------------------------------------- load
@@ -82,6 +87,7 @@ class BPEngine:
             tt = t if isinstance(t, torch.Tensor) else torch.from_numpy(np.asarray(t))
             o = int(L.node_off[v])
             self.T[o : o + tt.numel()] = tt.reshape(-1).to(L.device, self.dtype)
+        self._bf16_stale = True
 
     def load_messages(self, n2e_by_half: Sequence, e2n_by_half: Optional[Sequence] = None) -> None:
         L = self.layout
@@ -108,6 +114,7 @@ class BPEngine:
 
     def load_tensors_host(self, packed: torch.Tensor) -> None:
         self._staged(packed, self.T)
+        self._bf16_stale = True
 
     def load_messages_host(self, n2e: torch.Tensor, e2n: torch.Tensor) -> None:
         self._staged(n2e, self.n2e)
@@ -122,8 +129,12 @@ class BPEngine:
         ``mid_event`` (a torch.cuda.Event) is recorded between the node
         updates and the edge pass, to time the node-update kernel alone."""
         n2e_new, e2n_new = self._spare
+        if self.T_bf16 is not None and self._bf16_stale:
+            _lib.call("dqz_pack_bf16_planes", self.layout.gptr, self.T.data_ptr(), self.T_bf16.data_ptr(),
+                      _lib.stream_handle())
+            self._bf16_stale = False
         bp_sweep(self.layout, self.topo, self.T, self.n2e, self.e2n, n2e_new, e2n_new, mid_event,
-                 tensor_cores=self.precision == "bf16")
+                 T_bf16=self.T_bf16)
         self._spare = (self.n2e, self.e2n)
         self._prev = (self.n2e, self.e2n)
         self.n2e, self.e2n = n2e_new, e2n_new

@@ -116,13 +116,16 @@ class Topology:
                 else:
                     self.src_sel[h] = _lib.SRC_E2N_OLD
             level[v] = lv
-        self.levels = []
+        self.levels = []        # half-edges per level
+        self.node_levels = []   # nodes per level
         if self.nodes:
             for lv in range(int(level.max()) + 1):
                 vs = np.nonzero(level == lv)[0]
                 halves = np.concatenate([np.arange(self.node_half[v], self.node_half[v] + degree[v]) for v in vs])
                 self.levels.append(halves.astype(np.int32))
+                self.node_levels.append(vs.astype(np.int32))
         self._dev = None
+        self._dev_nodes = None
 
     def device_tables(self, device):
         if self._dev is None:
@@ -132,6 +135,11 @@ class Topology:
                 [torch.from_numpy(l).to(device) for l in self.levels],
             )
         return self._dev
+
+    def device_node_levels(self, device):
+        if self._dev_nodes is None:
+            self._dev_nodes = [torch.from_numpy(l).to(device) for l in self.node_levels]
+        return self._dev_nodes
 
     def half_ids(self):
         """(node, edge) element pairs of every half-edge, in half-edge order."""
@@ -165,28 +173,33 @@ def error_flag(device) -> torch.Tensor:
 
 
 def bp_sweep(layout: GraphLayout, topo: Topology, T, n2e_old, e2n_old, n2e_new, e2n_new, mid_event=None,
-             tensor_cores: bool = False):
+             T_bf16=None):
     """One sweep on packed arenas: node updates level by level, then the edge pass
     (``mid_event``, a torch.cuda.Event, is recorded between the two).
 
     complex128 arenas use the specialised degree-3 kernel when every node
     has that shape (layout.uniform_k3_chi), the generic kernel otherwise;
-    complex64 arenas need the specialised shape and run in FP32, or with
-    ``tensor_cores`` as BF16 tensor-core products with FP32 accumulation
-    (bonds of dimension 16)."""
+    complex64 arenas need the specialised shape and run in FP32, or, when
+    ``T_bf16`` (BF16 planes from dqz_pack_bf16_planes) is given, as BF16
+    tensor-core products with FP32 accumulation (bonds of dimension 16)."""
     src_sel, edge_new, levels = topo.device_tables(layout.device)
     stream = _lib.stream_handle()
     chi3 = layout.uniform_k3_chi()
     if T.dtype == torch.complex64:
-        if not chi3 or (tensor_cores and chi3 != 16):
+        if not chi3 or (T_bf16 is not None and chi3 != 16):
             raise NotImplementedError("complex64 BP needs degree-3 nodes with bonds of dimension 8 or 16 "
                                       "(16 for the tensor-core form)")
         flag = error_flag(layout.device)
-        code = 16 if tensor_cores else 32
-        for halves in levels:
-            _lib.call("dqz_bp_node_update_k3", layout.gptr, chi3, code, T.data_ptr(), n2e_old.data_ptr(),
-                      e2n_old.data_ptr(), n2e_new.data_ptr(), src_sel.data_ptr(), halves.data_ptr(), halves.numel(),
-                      flag.data_ptr(), stream)
+        if T_bf16 is not None:
+            for nodes in topo.device_node_levels(layout.device):
+                _lib.call("dqz_bp_node_update_k3_tc", layout.gptr, T_bf16.data_ptr(), n2e_old.data_ptr(),
+                          e2n_old.data_ptr(), n2e_new.data_ptr(), src_sel.data_ptr(), nodes.data_ptr(),
+                          nodes.numel(), flag.data_ptr(), stream)
+        else:
+            for halves in levels:
+                _lib.call("dqz_bp_node_update_k3", layout.gptr, chi3, 32, T.data_ptr(), n2e_old.data_ptr(),
+                          e2n_old.data_ptr(), n2e_new.data_ptr(), src_sel.data_ptr(), halves.data_ptr(),
+                          halves.numel(), flag.data_ptr(), stream)
         if mid_event is not None:
             mid_event.record(torch.cuda.current_stream())
         _lib.call("dqz_bp_edge_pass_c64", layout.gptr, n2e_old.data_ptr(), n2e_new.data_ptr(), edge_new.data_ptr(),

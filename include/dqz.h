@@ -98,6 +98,19 @@ int dqz_bp_node_update_k3(const dqz_graph_t *g, int32_t chi, int32_t precision, 
                           const uint8_t *src_sel, const int32_t *halves, int32_t n_halves,
                           int32_t *error_flag, cudaStream_t stream);
 
+/* Mixed-precision node update on tensor cores for the same shapes with
+ * chi = 16: BF16 products, FP32 accumulation, complex64 messages. One CTA per
+ * node (all three outgoing messages); `nodes` lists the nodes to update.
+ * `tensors_bf16` holds every node tensor as BF16 planes, node v at
+ * v * 16384 elements, [s][re|im][a][b][c], built by dqz_pack_bf16_planes. */
+int dqz_bp_node_update_k3_tc(const dqz_graph_t *g, const void *tensors_bf16, const void *n2e_old,
+                             const void *e2n_old, void *n2e_new, const uint8_t *src_sel,
+                             const int32_t *nodes, int32_t n_nodes, int32_t *error_flag,
+                             cudaStream_t stream);
+/* complex64 node tensors (node_off layout) -> BF16 planes for the kernel above. */
+int dqz_pack_bf16_planes(const dqz_graph_t *g, const void *tensors_c64, void *tensors_bf16,
+                         cudaStream_t stream);
+
 /* Edge pass on complex64 messages (see dqz_bp_edge_pass). */
 int dqz_bp_edge_pass_c64(const dqz_graph_t *g, const void *n2e_old, const void *n2e_new,
                          const uint8_t *edge_new, void *e2n_new, cudaStream_t stream);
