@@ -178,7 +178,7 @@ extern "C" int dqz_bp_node_update(const dqz_graph_t *g, const void *tensors, con
   if (use_scratch && !scratch) return DQZ_ERR_ARG;
   const size_t smem = bp_smem_bytes(max_slice, max_chi, use_scratch);
   if (smem > BP_SMEM_LIMIT) return DQZ_ERR_UNSUPPORTED;
-  cudaFuncSetAttribute(bp_node_generic, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)BP_SMEM_LIMIT);
+  DQZ_SMEM_ATTR_ONCE(bp_node_generic, BP_SMEM_LIMIT);
   int grid = use_scratch ? (n_halves < BP_SCRATCH_GRID ? n_halves : BP_SCRATCH_GRID) : n_halves;
   bp_node_generic<<<grid, BP_THREADS, smem, stream>>>(
       *g, (const cd *)tensors, (const cd *)n2e_old, (const cd *)e2n_old, (cd *)n2e_new, src_sel, halves, n_halves,

@@ -260,9 +260,7 @@ int launch_k3(const dqz_graph_t *g, const void *T, const void *n2e_old, const vo
               const uint8_t *src_sel, const int32_t *halves, int n_halves, int *error_flag, cudaStream_t stream) {
   const size_t smem = k3_smem<CHI, C>();
   if (smem > 227 * 1024) return DQZ_ERR_UNSUPPORTED;
-  if (cudaFuncSetAttribute(bp_node_k3<CHI, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
-      cudaSuccess)
-    return DQZ_ERR_CUDA;
+  DQZ_SMEM_ATTR_ONCE((bp_node_k3<CHI, C>), smem);
   bp_node_k3<CHI, C><<<n_halves, 32 * CHI, smem, stream>>>(*g, (const C *)T, (const C *)n2e_old,
                                                            (const C *)e2n_old, (C *)n2e_new, src_sel, halves,
                                                            n_halves, error_flag);

@@ -464,8 +464,7 @@ extern "C" int dqz_bp_node_update_k3_tc(const dqz_graph_t *g, const void *tensor
     return DQZ_ERR_ARG;
   if (n_nodes == 0) return DQZ_OK;
   const size_t smem = sizeof(TcSmem);
-  if (cudaFuncSetAttribute(bp_node_k3_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
-    return DQZ_ERR_CUDA;
+  DQZ_SMEM_ATTR_ONCE(bp_node_k3_tc, smem);
   bp_node_k3_tc<<<n_nodes, TC_THREADS, smem, stream>>>(*g, (const __nv_bfloat16 *)tensors_bf16,
                                                        (const float2 *)n2e_old, (const float2 *)e2n_old,
                                                        (float2 *)n2e_new, src_sel, nodes, n_nodes, error_flag);

@@ -128,3 +128,19 @@ __device__ __forceinline__ void mode_product(const cd *__restrict__ X, cd *__res
     cudaError_t _e = cudaGetLastError();                      \
     if (_e != cudaSuccess) return DQZ_ERR_CUDA;               \
   } while (0)
+
+// Raises a kernel's dynamic shared-memory limit once per device (the
+// attribute persists in the context), so that later launches -- including
+// launches recorded into a CUDA graph -- make no further attribute calls.
+#define DQZ_SMEM_ATTR_ONCE(kernel, bytes)                                                          \
+  do {                                                                                             \
+    static bool _dqz_attr_done[64] = {false};                                                      \
+    int _dqz_dev = 0;                                                                              \
+    if (cudaGetDevice(&_dqz_dev) != cudaSuccess || _dqz_dev < 0 || _dqz_dev >= 64) return DQZ_ERR_CUDA; \
+    if (!_dqz_attr_done[_dqz_dev]) {                                                               \
+      if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(bytes)) != \
+          cudaSuccess)                                                                             \
+        return DQZ_ERR_CUDA;                                                                       \
+      _dqz_attr_done[_dqz_dev] = true;                                                             \
+    }                                                                                              \
+  } while (0)

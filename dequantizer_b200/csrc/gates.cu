@@ -369,7 +369,7 @@ extern "C" int dqz_simple_update(const dqz_graph_t *g, void *tensors, double *la
   if (n == 0) return DQZ_OK;
   const size_t smem = su_smem_bytes(max_cols);
   if (smem > SMEM_LIMIT) return DQZ_ERR_UNSUPPORTED;
-  cudaFuncSetAttribute(simple_update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_LIMIT);
+  DQZ_SMEM_ATTR_ONCE(simple_update_kernel, SMEM_LIMIT);
   int grid = n < SU_GRID_MAX ? n : SU_GRID_MAX;
   simple_update_kernel<<<grid, GATE_THREADS, smem, stream>>>(*g, (cd *)tensors, lambdas, edges, ctrl_is_first,
                                                              (const cd *)halves, ranks, n, eps, max_rank, max_rows,

@@ -367,7 +367,7 @@ extern "C" int dqz_vidal_edges(const dqz_graph_t *g, const void *n2e, double eps
   const bool use_scratch = need > SMEM_LIMIT;
   if (use_scratch && !scratch) return DQZ_ERR_ARG;
   size_t smem = use_scratch ? eigh_smem(max_chi) : need;
-  cudaFuncSetAttribute(vidal_edges_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_LIMIT);
+  DQZ_SMEM_ATTR_ONCE(vidal_edges_kernel, SMEM_LIMIT);
   int grid = use_scratch ? (g->n_edges < SCRATCH_GRID ? g->n_edges : SCRATCH_GRID) : g->n_edges;
   vidal_edges_kernel<<<grid, GAUGE_THREADS, smem, stream>>>(*g, (const cd *)n2e, eps, (cd *)orth, lambdas, max_chi,
                                                            use_scratch ? (unsigned char *)scratch : nullptr);
@@ -389,7 +389,7 @@ extern "C" int dqz_absorb(const dqz_graph_t *g, const void *tensors_in, const vo
   size_t need = 48 * sizeof(double) + 2 * (size_t)max_size * sizeof(cd);
   const bool use_scratch = need > SMEM_LIMIT;
   if (use_scratch && !scratch) return DQZ_ERR_ARG;
-  cudaFuncSetAttribute(absorb_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_LIMIT);
+  DQZ_SMEM_ATTR_ONCE(absorb_kernel, SMEM_LIMIT);
   int grid = use_scratch ? (g->n_nodes < SCRATCH_GRID ? g->n_nodes : SCRATCH_GRID) : g->n_nodes;
   absorb_kernel<<<grid, GAUGE_THREADS, use_scratch ? 48 * sizeof(double) : need, stream>>>(
       *g, (const cd *)tensors_in, (const cd *)orth, (cd *)tensors_out, max_size,
@@ -405,7 +405,7 @@ extern "C" int dqz_vidal_distance(const dqz_graph_t *g, const void *tensors, con
   const int nh = g->n_halves;
   if (nh == 0 || g->n_edges == 0) return DQZ_ERR_ARG;
   size_t smem = eigh_smem(max_chi) + 2 * (size_t)max_chi * max_chi * sizeof(cd) + (size_t)max_chi * sizeof(double);
-  cudaFuncSetAttribute(vidal_distance_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_LIMIT);
+  DQZ_SMEM_ATTR_ONCE(vidal_distance_kernel, SMEM_LIMIT);
   vidal_distance_kernel<<<nh, GAUGE_THREADS, smem, stream>>>(*g, (const cd *)tensors, lambdas, eps, partial,
                                                              max_chi);
   DQZ_CHECK_LAUNCH();
@@ -448,7 +448,7 @@ extern "C" int dqz_density_matrices(const dqz_graph_t *g, const void *tensors, c
   size_t need = 2 * (size_t)max_size * sizeof(cd);
   const bool use_scratch = need > SMEM_LIMIT;
   if (use_scratch && !scratch) return DQZ_ERR_ARG;
-  cudaFuncSetAttribute(density_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_LIMIT);
+  DQZ_SMEM_ATTR_ONCE(density_kernel, SMEM_LIMIT);
   int grid = use_scratch ? (n_nodes < SCRATCH_GRID ? n_nodes : SCRATCH_GRID) : n_nodes;
   density_kernel<<<grid, GAUGE_THREADS, use_scratch ? 0 : need, stream>>>(
       *g, (const cd *)tensors, (const cd *)e2n, nodes, n_nodes, (cd *)rho, max_size,

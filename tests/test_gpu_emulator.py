@@ -177,6 +177,23 @@ def test_engine_bf16_meets_z_bound_at_fixed_point():
     assert np.abs(z["bf16"] - z["fp64"]).max() < 1e-4
 
 
+@pytest.mark.parametrize("precision,schedule", [("fp64", "async"), ("fp64", "sync"), ("bf16", "sync")])
+def test_graphed_sweeps_equal_eager_sweeps(precision, schedule):
+    """run_graphed replays captured blocks of sweeps: after the same number
+    of sweeps the messages equal the eager engine's bit for bit."""
+    g, tensors, m = _bench_like(24, 8)
+    engines = [BPEngine(g, schedule=schedule, precision=precision) for _ in range(2)]
+    for e in engines:
+        e.load_tensors(tensors)
+        e.load_messages([m] * e.layout.n_halves)
+    n = engines[1].run_graphed(0.0, max_sweeps=2 + 4 * 3, block=4)
+    assert n == 14
+    for _ in range(n):
+        engines[0].sweep()
+    assert torch.equal(engines[0].n2e, engines[1].n2e)
+    assert torch.equal(engines[0].e2n, engines[1].e2n)
+
+
 @pytest.mark.parametrize("schedule", ["sync", "async", "flooding"])
 def test_engine_sweeps_match_oracle(schedule):
     g = G.get_random_regular_graph(16, 3, 2, 4, 5)

@@ -1,0 +1,108 @@
+"""The example workloads on the GPU against the same loops run on the oracle.
+
+* 3-D Ising square-root network (examples/3d_ising_canonicalization.py:89-160):
+  same Vidal-distance history, iteration count and magnetisation.
+* Kicked Ising on the infinite heavy-hex cell (examples/ibm_eagle_processor.py:56-145).
+* Quantum annealing, first- and second-order Trotter steps
+  (examples/quantum_annealing/quantum_annealing/src/quantum_annealer.py:90-152).
+Tolerances: 1e-9 on magnetisations / <Z> / density matrices (FP64 on both
+sides, the same BP schedule and the same seeded messages).
+"""
+
+import numpy as np
+import pytest
+
+from dequantizer_b200 import workloads as W
+from dequantizer_b200 import graph as G
+from dequantizer_b200.graph import Edge, Node
+from dequantizer_b200.initializers import get_message_random_nonnegative_initializer, get_potts_initializer
+from oracle import maps as OM
+from oracle.emulator import BPQuantumEmulator as OracleEmulator
+
+pytestmark = pytest.mark.gpu
+
+
+def oracle_ising(sizes, betas, coupling, field, accuracy, key=42):
+    lat = G.get_nd_lattice(list(sizes), 2, 2, True)
+    trav = list(lat.get_traversal_iterator(ordering="dfs"))
+    bp = OM.get_belief_propagation_map(trav)
+    vg = OM.get_vidal_gauge_fixing_map(trav, accuracy)
+    vd = OM.get_vidal_gauge_distance_map(trav, accuracy)
+    spins = np.array([1.0, -1.0])
+    out = []
+    for beta in betas:
+        init = get_potts_initializer(np.exp(-coupling * beta * np.tensordot(spins, spins, axes=0)),
+                                     np.exp(-field * beta * spins))
+        tensors = OM.init_tensors(lat, init)
+        msgs = lat.init_messages(get_message_random_nonnegative_initializer(key))
+        hist, d = [], np.finfo(np.float64).max
+        while d > accuracy:
+            msgs = bp(tensors, msgs)
+            t, l = vg(tensors, msgs)
+            d = vd(t, l)
+            hist.append(d)
+        mag = np.mean([2 * OM.get_one_side_density_matrix(el, tensors, msgs)[0, 0].real - 1
+                       for el in trav if isinstance(el, Node)])
+        out.append((hist, mag))
+    return out
+
+
+@pytest.mark.parametrize("field", [0.5, 0.0])
+def test_ising_sqrt_partition_matches_oracle(field):
+    betas = [0.1, 0.4]
+    res = W.ising_sqrt_partition([3, 3, 3], betas, coupling=-1.0, field_strength=field, accuracy=1e-9)
+    ref = oracle_ising([3, 3, 3], betas, -1.0, field, 1e-9)
+    for i, (hist, mag) in enumerate(ref):
+        assert res.number_of_iterations[i] == len(hist)
+        assert np.abs(res.vidal_dist_per_iter[i] - np.array(hist)).max() < 1e-9
+        assert abs(res.average_magnetization[i] - mag) < 1e-9
+
+
+def test_kicked_ising_infinite_cell_matches_oracle():
+    z_gpu, _ = W.run_eagle_simulation(max_chi=8, layers_per_regauging=1, trotter_steps=3, accuracy=1e-7,
+                                      theta=0.8, is_infinite=True, max_belief_propagation_iterations=100)
+    lat = G.get_heavy_hex_ibm_eagle_lattice_infinite()
+    trav = list(lat.get_traversal_iterator())
+    em = OracleEmulator(lat, 42, 8, lat.edges_number, 1e-7, 100)
+    rzz, rx = W.kicked_ising_gates(0.8)
+    z_ref = [float((em.dens_q1(2)[0, 0] - em.dens_q1(2)[1, 1]).real)]
+    for _ in range(3):
+        for nid in range(lat.nodes_number):
+            em.apply_q1(rx, nid)
+        for el in trav:
+            if isinstance(el, Edge):
+                em.apply_q2(rzz, *el.id)
+        rho = em.dens_q1(2)
+        z_ref.append(float((rho[0, 0] - rho[1, 1]).real))
+    assert np.abs(np.array(z_gpu) - np.array(z_ref)).max() < 1e-9
+
+
+@pytest.mark.parametrize("second_order", [False, True])
+def test_annealing_matches_oracle(second_order):
+    energy = W.random_regular_energy(10, 3, seed=4, field_std=0.5)
+    steps = list(W.scheduler(0.2, lambda t: 1 - t, 6))
+    res = W.run_quantum_annealer(energy, steps, key=7, max_chi=4, gates_number_per_regauging=energy.edges_number,
+                                 accuracy=1e-7, max_belief_propagation_iterations=100,
+                                 second_order=second_order)
+    g = W.tensor_graph_of(energy)
+    em = OracleEmulator(g, 7, 4, energy.edges_number, 1e-7, 100)
+    n = g.nodes_number
+    deg = {nid: g.get_node(nid).degree for nid in g.nodes}
+    for nid in range(n):
+        em.apply_q1(W.HADAMARD, nid)
+    for mix, coup in steps:
+        if second_order:
+            for nid in range(n):
+                em.apply_q1(W.q1_gate(mix / 2), nid)
+        for (a, b), J in zip(energy.coupled_spin_pairs, energy.coupling_amplitudes):
+            a, b = int(a), int(b)
+            em.apply_q2(W.q2_gate(J, energy.fields[a] / deg[a], energy.fields[b] / deg[b], coup), a, b)
+        for nid in range(n):
+            em.apply_q1(W.q1_gate(mix / 2 if second_order else mix), nid)
+    rho_ref = np.stack([em.dens_q1(i) for i in range(n)])
+    assert np.abs(res.density_matrices - rho_ref).max() < 1e-9
+    assert np.abs(res.truncation_errors - np.array(em.truncation_errors)).max() < 1e-9
+    assert np.abs(res.entropies - np.array(em.entropies)).max() < 1e-9
+    assert np.abs(res.vidal_distances_after_regauging - np.array(em.after_regauging_vidal_distances)).max() < 1e-9
+    spins = 2 * (res.density_matrices[:, 0, 0].real > 0.5) - 1
+    assert np.isfinite(W.eval_energy(energy, spins))
