@@ -86,11 +86,11 @@ _SIGNATURES = {
     "dqz_messages_distance": (ctypes.c_int, [_G, _P, _P, _P, _P, _P, _P, _I, _P]),
     "dqz_reduce_sum": (ctypes.c_int, [_P, _I, _D, _P, _P]),
     "dqz_segment_distance": (ctypes.c_int, [_P, _P, _P, _I, _P, _P, _P]),
-    "dqz_vidal_edges": (ctypes.c_int, [_G, _P, _D, _P, _P, _I, _P, _P]),
+    "dqz_vidal_edges": (ctypes.c_int, [_G, _P, _D, _P, _P, _I, _P, _I, _P, _P]),
     "dqz_vidal_edges_scratch_bytes": (_S, [_I, _I]),
-    "dqz_absorb": (ctypes.c_int, [_G, _P, _P, _P, _I, _P, _P]),
+    "dqz_absorb": (ctypes.c_int, [_G, _P, _P, _P, _I, _P, _I, _P, _P]),
     "dqz_absorb_scratch_bytes": (_S, [_I, _I]),
-    "dqz_vidal_distance": (ctypes.c_int, [_G, _P, _P, _D, _P, _P, _I, _P]),
+    "dqz_vidal_distance": (ctypes.c_int, [_G, _P, _P, _D, _P, _P, _I, _I, _P, _I, _P]),
     "dqz_symmetric_gauge": (ctypes.c_int, [_G, _P, _P, _D, _P, _P]),
     "dqz_lambdas_to_messages": (ctypes.c_int, [_G, _P, _P, _P, _I, _P]),
     "dqz_density_matrices": (ctypes.c_int, [_G, _P, _P, _P, _I, _P, _I, _P, _P]),

@@ -1,7 +1,12 @@
 // Gauge kernels (FP64 / complex128):
-//  * vidal_edges    -- tensor_ops.py:108-130 (edge_svd), one CTA per edge
+//  * vidal_edges    -- tensor_ops.py:108-130 (edge_svd): one warp per edge for
+//                      chi <= 16, one CTA per edge above
 //  * absorb         -- tensor_ops.py:88-93 (absorb_by_node), one CTA per node
-//  * vidal_distance -- tensor_ops.py:143-175 + mappings/vidal_distance.py:17-42
+//  * vidal_distance -- tensor_ops.py:143-175 + mappings/vidal_distance.py:17-42:
+//                      one warp per half-edge for chi <= 16 and bond slices of
+//                      <= 1024 entries, one CTA per half-edge above
+// vidal_edges, absorb and vidal_distance take an optional list of the
+// edges / nodes / half-edges to process (null = all).
 //  * symmetric      -- tensor_ops.py:189-199 (canonicalize)
 //  * lambdas->msgs  -- mappings/symmetric_gauge.py:50-61
 //  * density        -- mappings/density_matrix.py:16-37
@@ -13,6 +18,10 @@ namespace {
 
 constexpr int GAUGE_THREADS = 256;
 constexpr size_t SMEM_LIMIT = 200 * 1024;
+constexpr int WARP_MAX_CHI = 16;     // largest bond of the one-warp kernels
+constexpr int WARP_MAX_SLICE = 1024; // largest bond slice (size / chi) of the one-warp distance kernel
+constexpr int WARP_ROTS = 17;        // rotation slots per warp (n / 2 + 1 for n <= 32)
+constexpr size_t WARP_BLOCK_SMEM = 96 * 1024;
 constexpr int SCRATCH_GRID = 148 * 4;
 const double F32_MAX = 3.4028234663852886e38;
 
@@ -26,9 +35,12 @@ __host__ __device__ inline size_t vidal_edge_bytes(int c) {
   return 8 * (size_t)c * c * sizeof(cd) + 3 * (size_t)c * sizeof(double) + 2 * (size_t)c * sizeof(int) + 64;
 }
 
+__host__ __device__ inline size_t round16(size_t x) { return (x + 15) & ~(size_t)15; }
+
 __global__ void __launch_bounds__(GAUGE_THREADS) vidal_edges_kernel(dqz_graph_t g, const cd *__restrict__ n2e,
                                                                      double eps, cd *orth, double *lambdas,
-                                                                     int max_chi, unsigned char *scratch) {
+                                                                     int max_chi, unsigned char *scratch,
+                                                                     const int32_t *__restrict__ sel, int n_sel) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double *red = reinterpret_cast<double *>(smem_raw);
   Rot *rots = reinterpret_cast<Rot *>(smem_raw + 48 * sizeof(double));
@@ -43,7 +55,9 @@ __global__ void __launch_bounds__(GAUGE_THREADS) vidal_edges_kernel(dqz_graph_t 
   int *perm = reinterpret_cast<int *>(sv + max_chi);
   const int tid = threadIdx.x, nt = blockDim.x;
 
-  for (int e = blockIdx.x; e < g.n_edges; e += gridDim.x) {
+  const int total = sel ? n_sel : g.n_edges;
+  for (int it = blockIdx.x; it < total; it += gridDim.x) {
+    const int e = sel ? sel[it] : it;
     const int h0 = g.edge_half[2 * e], h1 = g.edge_half[2 * e + 1];
     const int c = g.edge_chi[e];
     const cd *mf = n2e + g.half_msg_off[h0];
@@ -123,16 +137,124 @@ __global__ void __launch_bounds__(GAUGE_THREADS) vidal_edges_kernel(dqz_graph_t 
   }
 }
 
+// One warp per edge (chi <= WARP_MAX_CHI): the same steps as
+// vidal_edges_kernel on the warp's own slice of shared memory.
+__host__ __device__ inline size_t warp_edge_bytes(int c) {
+  return round16(WARP_ROTS * sizeof(Rot)) + round16(vidal_edge_bytes(c));
+}
+
+__global__ void __launch_bounds__(GAUGE_THREADS) vidal_edges_warp_kernel(dqz_graph_t g, const cd *__restrict__ n2e,
+                                                                          double eps, cd *orth, double *lambdas,
+                                                                          int max_chi,
+                                                                          const int32_t *__restrict__ sel, int n_sel) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, wpb = blockDim.x >> 5;
+  unsigned char *wbase = smem_raw + (size_t)wid * warp_edge_bytes(max_chi);
+  Rot *rots = reinterpret_cast<Rot *>(wbase);
+  unsigned char *base = wbase + round16(WARP_ROTS * sizeof(Rot));
+  const int M2 = max_chi * max_chi;
+  cd *Af = reinterpret_cast<cd *>(base);
+  cd *Vf = Af + M2, *Ab = Vf + M2, *Vb = Ab + M2, *Qf = Vb + M2, *Qb = Qf + M2, *C = Qb + M2, *W = C + M2;
+  double *wf = reinterpret_cast<double *>(W + M2);
+  double *wb = wf + max_chi, *sv = wb + max_chi;
+  int *perm = reinterpret_cast<int *>(sv + max_chi);
+  const int total = sel ? n_sel : g.n_edges;
+  for (int it = blockIdx.x * wpb + wid; it < total; it += gridDim.x * wpb) {
+    const int e = sel ? sel[it] : it;
+    const int h0 = g.edge_half[2 * e], h1 = g.edge_half[2 * e + 1];
+    const int c = g.edge_chi[e];
+    double *lam = lambdas + g.edge_lam_off[e];
+    if (c > max_chi) {  // the caller's max_chi is below this bond: flag it
+      if (lane == 0) lam[0] = __longlong_as_double(0x7ff8000000000000ll);
+      continue;
+    }
+    const cd *mf = n2e + g.half_msg_off[h0];
+    const cd *mb = n2e + g.half_msg_off[h1];
+    for (int i = lane; i < c * c; i += 32) {
+      Af[i] = mf[i];
+      Ab[i] = mb[i];
+    }
+    __syncwarp();
+    warp_herm_eigh(Af, c, Vf, c, c, wf, rots);
+    warp_herm_eigh(Ab, c, Vb, c, c, wb, rots);
+    for (int idx = lane; idx < c * c; idx += 32) {
+      const int i = idx / c, j = idx % c;
+      cd sf = czero(), sif = czero(), sb = czero(), sib = czero();
+      for (int k = 0; k < c; ++k) {
+        cd pf = cmul(Vf[i * c + k], cconj(Vf[j * c + k]));
+        cd pb = cmul(Vb[i * c + k], cconj(Vb[j * c + k]));
+        sf = cadd(sf, cscale(pf, sqrt(safe_truncate(wf[k], eps))));
+        sif = cadd(sif, cscale(pf, sqrt(safe_inverse(wf[k], eps))));
+        sb = cadd(sb, cscale(pb, sqrt(safe_truncate(wb[k], eps))));
+        sib = cadd(sib, cscale(pb, sqrt(safe_inverse(wb[k], eps))));
+      }
+      Af[idx] = sf;
+      Qf[idx] = sif;
+      Ab[idx] = sb;
+      Qb[idx] = sib;
+    }
+    __syncwarp();
+    // C = sqrt(m_f) sqrt(m_b)^T, column-major for the one-sided Jacobi.
+    for (int idx = lane; idx < c * c; idx += 32) {
+      const int i = idx / c, j = idx % c;
+      cd acc = czero();
+      for (int k = 0; k < c; ++k) cfma(acc, Af[i * c + k], Ab[j * c + k]);
+      C[j * c + i] = acc;
+    }
+    __syncwarp();
+    warp_hestenes(C, c, c, c, W, c, sv);
+    warp_sort_desc(sv, c, perm);
+    double nrm2 = 0.0;
+    for (int j = lane; j < c; j += 32) nrm2 += sv[j] * sv[j];
+    nrm2 = warp_sum(nrm2);
+    const double inv_n = 1.0 / sqrt(nrm2);
+    for (int j = lane; j < c; j += 32) lam[j] = safe_truncate(sv[perm[j]] * inv_n, eps);
+    __syncwarp();
+    double un = 0.0, vn = 0.0;
+    for (int idx = lane; idx < c * c; idx += 32) {
+      const int i = idx / c, j = idx % c;
+      const int pj = perm[j];
+      const bool keep = lam[j] > eps && sv[pj] > 0.0;
+      cd u = keep ? cscale(C[pj * c + i], 1.0 / sv[pj]) : czero();
+      cd w = keep ? cconj(W[pj * c + i]) : czero();
+      Af[i * c + j] = u;
+      Ab[i * c + j] = w;
+      un += cabs2(u);
+      vn += cabs2(w);
+    }
+    un = warp_sum(un);
+    vn = warp_sum(vn);
+    __syncwarp();
+    const double iu = 1.0 / sqrt(un), iv = 1.0 / sqrt(vn);
+    cd *Gf = orth + g.half_msg_off[h0];
+    cd *Gb = orth + g.half_msg_off[h1];
+    for (int idx = lane; idx < c * c; idx += 32) {
+      const int i = idx / c, j = idx % c;
+      cd af = czero(), ab = czero();
+      for (int k = 0; k < c; ++k) {
+        cfma(af, Qf[i * c + k], Af[k * c + j]);
+        cfma(ab, Qb[i * c + k], Ab[k * c + j]);
+      }
+      Gf[idx] = cscale(af, iu);
+      Gb[idx] = cscale(ab, iv);
+    }
+    __syncwarp();
+  }
+}
+
 // ----------------------------------------------------------------- absorb
 __global__ void __launch_bounds__(GAUGE_THREADS) absorb_kernel(dqz_graph_t g, const cd *__restrict__ Tin,
                                                                 const cd *__restrict__ orth, cd *Tout, int max_size,
-                                                                cd *scratch) {
+                                                                cd *scratch, const int32_t *__restrict__ sel,
+                                                                int n_sel) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double *red = reinterpret_cast<double *>(smem_raw);
   cd *bufA = scratch ? scratch + (long long)blockIdx.x * 2 * max_size
                      : reinterpret_cast<cd *>(smem_raw + 48 * sizeof(double));
   cd *bufB = bufA + max_size;
-  for (int v = blockIdx.x; v < g.n_nodes; v += gridDim.x) {
+  const int total = sel ? n_sel : g.n_nodes;
+  for (int it = blockIdx.x; it < total; it += gridDim.x) {
+    const int v = sel ? sel[it] : it;
     NodeShape s;
     load_shape(g, v, s);
     const cd *T = Tin + g.node_off[v];
@@ -166,7 +288,8 @@ __global__ void __launch_bounds__(GAUGE_THREADS) absorb_kernel(dqz_graph_t g, co
 // partial[h] = trace norm of (R/tr R - ideal) for bond e of node v (h = (v,e)).
 __global__ void __launch_bounds__(GAUGE_THREADS) vidal_distance_kernel(dqz_graph_t g, const cd *__restrict__ Tall,
                                                                         const double *__restrict__ lambdas,
-                                                                        double eps, double *partial, int max_chi) {
+                                                                        double eps, double *partial, int max_chi,
+                                                                        const int32_t *__restrict__ sel, int n_sel) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double *red = reinterpret_cast<double *>(smem_raw);
   Rot *rots = reinterpret_cast<Rot *>(smem_raw + 48 * sizeof(double));
@@ -175,9 +298,10 @@ __global__ void __launch_bounds__(GAUGE_THREADS) vidal_distance_kernel(dqz_graph
   double *w = reinterpret_cast<double *>(Vm + max_chi * max_chi);
   __shared__ cd trace_sh;
   __shared__ int count_sh;
-  const int nh = g.n_halves;
+  const int total = sel ? n_sel : g.n_halves;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  for (int h = blockIdx.x; h < nh; h += gridDim.x) {
+  for (int it = blockIdx.x; it < total; it += gridDim.x) {
+    const int h = sel ? sel[it] : it;
     const int v = g.half_node[h];
     NodeShape s;
     load_shape(g, v, s);
@@ -242,6 +366,95 @@ __global__ void __launch_bounds__(GAUGE_THREADS) vidal_distance_kernel(dqz_graph
     t = block_sum(t, red);
     if (threadIdx.x == 0) partial[h] = t;
     __syncthreads();
+  }
+}
+
+// One warp per half-edge (chi <= WARP_MAX_CHI, bond slice <= max_slice <=
+// WARP_MAX_SLICE): the lambda^2 weight of every slice entry is formed once in
+// shared memory, each lane accumulates entries (a', a >= a') of R over the
+// slice, and the trace norm comes from warp_herm_eigh.
+__host__ __device__ inline size_t warp_vd_bytes(int c, int max_slice) {
+  return round16(WARP_ROTS * sizeof(Rot)) + round16((size_t)c * c * sizeof(cd)) + round16((size_t)c * sizeof(double)) +
+         round16((size_t)max_slice * sizeof(double));
+}
+
+__global__ void __launch_bounds__(GAUGE_THREADS) vidal_distance_warp_kernel(
+    dqz_graph_t g, const cd *__restrict__ Tall, const double *__restrict__ lambdas, double eps, double *partial,
+    int max_chi, int max_slice, const int32_t *__restrict__ sel, int n_sel) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, wpb = blockDim.x >> 5;
+  unsigned char *wbase = smem_raw + (size_t)wid * warp_vd_bytes(max_chi, max_slice);
+  Rot *rots = reinterpret_cast<Rot *>(wbase);
+  cd *Rm = reinterpret_cast<cd *>(wbase + round16(WARP_ROTS * sizeof(Rot)));
+  double *wv = reinterpret_cast<double *>(reinterpret_cast<unsigned char *>(Rm) +
+                                          round16((size_t)max_chi * max_chi * sizeof(cd)));
+  double *wx = reinterpret_cast<double *>(reinterpret_cast<unsigned char *>(wv) +
+                                          round16((size_t)max_chi * sizeof(double)));
+  const int total = sel ? n_sel : g.n_halves;
+  for (int it = blockIdx.x * wpb + wid; it < total; it += gridDim.x * wpb) {
+    const int h = sel ? sel[it] : it;
+    const int v = g.half_node[h];
+    NodeShape s;
+    load_shape(g, v, s);
+    const int e = h - s.half0;
+    const int ce = s.dims[e];
+    const long long P64 = s.size / ce;
+    if (ce > max_chi || P64 > max_slice) {  // outside the caller's bounds: flag it
+      if (lane == 0) partial[h] = __longlong_as_double(0x7ff8000000000000ll);
+      continue;
+    }
+    const int P = (int)P64, Re = (int)s.stride[e];
+    const cd *T = Tall + g.node_off[v];
+    for (int x = lane; x < P; x += 32) {
+      const int l = x / Re, r = x - l * Re;
+      const int o0 = l * ce * Re + r;  // offset with a_e = 0
+      double wt = 1.0;
+      for (int f = 0; f < s.k; ++f) {
+        if (f == e) continue;
+        const int idx = (o0 / (int)s.stride[f]) % s.dims[f];
+        const double lv = lambdas[g.edge_lam_off[g.half_edge[s.half0 + f]] + idx];
+        wt *= lv * lv;
+      }
+      wx[x] = wt;
+    }
+    __syncwarp();
+    const int npair = ce * (ce + 1) / 2;
+    const int nblk = P / Re;
+    for (int pi = lane; pi < npair; pi += 32) {
+      int ap = 0, rem = pi;
+      while (rem >= ce - ap) {
+        rem -= ce - ap;
+        ++ap;
+      }
+      const int a = ap + rem;
+      const cd *Tp = T + (long long)ap * Re, *Ta = T + (long long)a * Re;
+      cd acc = czero();
+      int x = 0;
+      for (int l = 0; l < nblk; ++l) {
+        const int o = l * ce * Re;
+        for (int r = 0; r < Re; ++r, ++x) cfmac(acc, Tp[o + r], cscale(Ta[o + r], wx[x]));
+      }
+      Rm[ap * ce + a] = acc;
+      Rm[a * ce + ap] = cconj(acc);
+    }
+    __syncwarp();
+    cd tr = czero();
+    for (int i = 0; i < ce; ++i) tr = cadd(tr, Rm[i * ce + i]);
+    int cnt = 0;
+    for (int i = 0; i < ce; ++i) cnt += cdiv(Rm[i * ce + i], tr).x > eps ? 1 : 0;
+    __syncwarp();
+    for (int i = lane; i < ce * ce; i += 32) Rm[i] = cdiv(Rm[i], tr);
+    __syncwarp();
+    const double idv = 1.0 / (double)cnt;
+    for (int i = lane; i < ce; i += 32)
+      if (Rm[i * ce + i].x > eps) Rm[i * ce + i].x -= idv;
+    __syncwarp();
+    warp_herm_eigh(Rm, ce, nullptr, 0, ce, wv, rots);
+    double t = 0.0;
+    for (int i = lane; i < ce; i += 32) t += fabs(wv[i]);
+    t = warp_sum(t);
+    if (lane == 0) partial[h] = t;
+    __syncwarp();
   }
 }
 
@@ -359,18 +572,32 @@ extern "C" size_t dqz_vidal_edges_scratch_bytes(int32_t n_edges, int32_t max_chi
 }
 
 extern "C" int dqz_vidal_edges(const dqz_graph_t *g, const void *n2e, double eps, void *orth, double *lambdas,
-                               int32_t max_chi, void *scratch, cudaStream_t stream) {
+                               int32_t max_chi, const int32_t *edges, int32_t n_sel, void *scratch,
+                               cudaStream_t stream) {
   if (!g || !n2e || !orth || !lambdas) return DQZ_ERR_ARG;
   if (max_chi <= 0 || max_chi > DQZ_MAX_CHI) return DQZ_ERR_UNSUPPORTED;
-  if (g->n_edges == 0) return DQZ_OK;
+  if (edges && (n_sel < 0 || n_sel > g->n_edges)) return DQZ_ERR_ARG;
+  const int total = edges ? n_sel : g->n_edges;
+  if (total == 0) return DQZ_OK;
+  if (max_chi <= WARP_MAX_CHI) {
+    const size_t per = warp_edge_bytes(max_chi);
+    int wpb = (int)(WARP_BLOCK_SMEM / per);
+    wpb = wpb < 1 ? 1 : (wpb > GAUGE_THREADS / 32 ? GAUGE_THREADS / 32 : wpb);
+    DQZ_SMEM_ATTR_ONCE(vidal_edges_warp_kernel, SMEM_LIMIT);
+    vidal_edges_warp_kernel<<<(total + wpb - 1) / wpb, 32 * wpb, wpb * per, stream>>>(
+        *g, (const cd *)n2e, eps, (cd *)orth, lambdas, max_chi, edges, total);
+    DQZ_CHECK_LAUNCH();
+    return DQZ_OK;
+  }
   size_t need = eigh_smem(max_chi) + vidal_edge_bytes(max_chi);
   const bool use_scratch = need > SMEM_LIMIT;
   if (use_scratch && !scratch) return DQZ_ERR_ARG;
   size_t smem = use_scratch ? eigh_smem(max_chi) : need;
   DQZ_SMEM_ATTR_ONCE(vidal_edges_kernel, SMEM_LIMIT);
-  int grid = use_scratch ? (g->n_edges < SCRATCH_GRID ? g->n_edges : SCRATCH_GRID) : g->n_edges;
+  int grid = use_scratch ? (total < SCRATCH_GRID ? total : SCRATCH_GRID) : total;
   vidal_edges_kernel<<<grid, GAUGE_THREADS, smem, stream>>>(*g, (const cd *)n2e, eps, (cd *)orth, lambdas, max_chi,
-                                                           use_scratch ? (unsigned char *)scratch : nullptr);
+                                                           use_scratch ? (unsigned char *)scratch : nullptr, edges,
+                                                           total);
   DQZ_CHECK_LAUNCH();
   return DQZ_OK;
 }
@@ -383,32 +610,50 @@ extern "C" size_t dqz_absorb_scratch_bytes(int32_t n_nodes, int32_t max_size) {
 }
 
 extern "C" int dqz_absorb(const dqz_graph_t *g, const void *tensors_in, const void *orth, void *tensors_out,
-                          int32_t max_size, void *scratch, cudaStream_t stream) {
+                          int32_t max_size, const int32_t *nodes, int32_t n_sel, void *scratch,
+                          cudaStream_t stream) {
   if (!g || !tensors_in || !orth || !tensors_out || max_size <= 0) return DQZ_ERR_ARG;
-  if (g->n_nodes == 0) return DQZ_OK;
+  if (nodes && (n_sel < 0 || n_sel > g->n_nodes)) return DQZ_ERR_ARG;
+  const int total = nodes ? n_sel : g->n_nodes;
+  if (total == 0) return DQZ_OK;
   size_t need = 48 * sizeof(double) + 2 * (size_t)max_size * sizeof(cd);
   const bool use_scratch = need > SMEM_LIMIT;
   if (use_scratch && !scratch) return DQZ_ERR_ARG;
   DQZ_SMEM_ATTR_ONCE(absorb_kernel, SMEM_LIMIT);
-  int grid = use_scratch ? (g->n_nodes < SCRATCH_GRID ? g->n_nodes : SCRATCH_GRID) : g->n_nodes;
+  int grid = use_scratch ? (total < SCRATCH_GRID ? total : SCRATCH_GRID) : total;
   absorb_kernel<<<grid, GAUGE_THREADS, use_scratch ? 48 * sizeof(double) : need, stream>>>(
       *g, (const cd *)tensors_in, (const cd *)orth, (cd *)tensors_out, max_size,
-      use_scratch ? (cd *)scratch : nullptr);
+      use_scratch ? (cd *)scratch : nullptr, nodes, total);
   DQZ_CHECK_LAUNCH();
   return DQZ_OK;
 }
 
 extern "C" int dqz_vidal_distance(const dqz_graph_t *g, const void *tensors, const double *lambdas, double eps,
-                                  double *partial, double *out, int32_t max_chi, cudaStream_t stream) {
-  if (!g || !tensors || !lambdas || !partial || !out) return DQZ_ERR_ARG;
+                                  double *partial, double *out, int32_t max_chi, int32_t max_slice,
+                                  const int32_t *halves, int32_t n_sel, cudaStream_t stream) {
+  if (!g || !tensors || !lambdas || !partial) return DQZ_ERR_ARG;
   if (max_chi <= 0 || max_chi > DQZ_MAX_CHI) return DQZ_ERR_UNSUPPORTED;
   const int nh = g->n_halves;
   if (nh == 0 || g->n_edges == 0) return DQZ_ERR_ARG;
-  size_t smem = eigh_smem(max_chi) + 2 * (size_t)max_chi * max_chi * sizeof(cd) + (size_t)max_chi * sizeof(double);
-  DQZ_SMEM_ATTR_ONCE(vidal_distance_kernel, SMEM_LIMIT);
-  vidal_distance_kernel<<<nh, GAUGE_THREADS, smem, stream>>>(*g, (const cd *)tensors, lambdas, eps, partial,
-                                                             max_chi);
-  DQZ_CHECK_LAUNCH();
+  if (halves && (n_sel < 0 || n_sel > nh)) return DQZ_ERR_ARG;
+  const int total = halves ? n_sel : nh;
+  if (total > 0) {
+    if (max_chi <= WARP_MAX_CHI && max_slice > 0 && max_slice <= WARP_MAX_SLICE) {
+      const size_t per = warp_vd_bytes(max_chi, max_slice);
+      int wpb = (int)(WARP_BLOCK_SMEM / per);
+      wpb = wpb < 1 ? 1 : (wpb > GAUGE_THREADS / 32 ? GAUGE_THREADS / 32 : wpb);
+      DQZ_SMEM_ATTR_ONCE(vidal_distance_warp_kernel, SMEM_LIMIT);
+      vidal_distance_warp_kernel<<<(total + wpb - 1) / wpb, 32 * wpb, wpb * per, stream>>>(
+          *g, (const cd *)tensors, lambdas, eps, partial, max_chi, max_slice, halves, total);
+    } else {
+      size_t smem = eigh_smem(max_chi) + 2 * (size_t)max_chi * max_chi * sizeof(cd) + (size_t)max_chi * sizeof(double);
+      DQZ_SMEM_ATTR_ONCE(vidal_distance_kernel, SMEM_LIMIT);
+      vidal_distance_kernel<<<total, GAUGE_THREADS, smem, stream>>>(*g, (const cd *)tensors, lambdas, eps, partial,
+                                                                    max_chi, halves, total);
+    }
+    DQZ_CHECK_LAUNCH();
+  }
+  if (!out) return DQZ_OK;
   return dqz_reduce_sum(partial, nh, 1.0 / (2.0 * g->n_edges), out, stream);
 }
 

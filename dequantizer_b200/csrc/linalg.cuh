@@ -6,6 +6,8 @@
 //                  SVDs of tensor_ops.py:121 and :360.
 //  * householder_qr / apply_q -- LAPACK-convention (zgeqr2 / zung2r) QR, the
 //                  QR of tensor_ops.py:288.
+//  * warp_herm_eigh / warp_hestenes / warp_sort_desc -- one-warp forms of the
+//                  above for matrices up to 32 x 32.
 // Pairs are scheduled with the round-robin (circle) ordering, so each step
 // rotates n/2 disjoint index pairs at once.
 #pragma once
@@ -59,23 +61,42 @@ __device__ __forceinline__ bool jacobi_rot(double a, double b, cd c, Rot &r) {
 // return w[i] holds eigenvalue i and column i of V (row-major, ldv) the
 // matching eigenvector (unsorted). rots: >= n/2+1 entries, red: 33 doubles,
 // all in shared memory.
+// The input is first made exactly Hermitian ((A + A^H) / 2, real diagonal):
+// an anti-Hermitian rounding residual is invisible to the rotations, which
+// read the upper triangle only, and would otherwise keep the off-diagonal
+// norm above any relative stopping threshold. Convergence is measured on the
+// upper triangle; a sweep that rotates nothing also ends the iteration.
 static __device__ void herm_eigh(cd *A, int lda, cd *V, int ldv, int n, double *w, Rot *rots, double *red,
                           int max_sweeps = 40) {
   const int tid = threadIdx.x, nt = blockDim.x;
+  __shared__ int rotated_sh;
   for (int i = tid; i < n * n; i += nt) V[(i / n) * ldv + (i % n)] = (i / n == i % n) ? mk(1.0, 0.0) : czero();
+  for (int i = tid; i < n * n; i += nt) {
+    const int r = i / n, c = i % n;
+    if (r < c) {
+      const cd u = A[r * lda + c], l = A[c * lda + r];
+      const cd h = mk(0.5 * (u.x + l.x), 0.5 * (u.y - l.y));
+      A[r * lda + c] = h;
+      A[c * lda + r] = cconj(h);
+    } else if (r == c) {
+      A[r * lda + c].y = 0.0;
+    }
+  }
   __syncthreads();
   const int np = n + (n & 1);
   const int npairs = np / 2;
   if (n > 1) {
     for (int sweep = 0; sweep < max_sweeps; ++sweep) {
+      // reset before the barriers inside block_sum; read after the last step
+      if (tid == 0) rotated_sh = 0;
       double off = 0.0, dia = 0.0;
       for (int i = tid; i < n * n; i += nt) {
         int r = i / n, c = i % n;
         double v = cabs2(A[r * lda + c]);
         if (r == c)
           dia += v;
-        else
-          off += v;
+        else if (r < c)
+          off += 2.0 * v;
       }
       off = block_sum(off, red);
       dia = block_sum(dia, red);
@@ -91,7 +112,10 @@ static __device__ void herm_eigh(cd *A, int lda, cd *V, int ldv, int n, double *
             double a = A[p * lda + p].x, b = A[q * lda + q].x;
             cd c = A[p * lda + q];
             double ac2 = cabs2(c);
-            if (ac2 > 0.0 && ac2 >= 1e-36 * (a * a + b * b) && jacobi_rot(a, b, c, r)) r.p = p;
+            if (ac2 > 0.0 && ac2 >= 1e-36 * (a * a + b * b) && jacobi_rot(a, b, c, r)) {
+              r.p = p;
+              rotated_sh = 1;
+            }
           }
           rots[i] = r;
         }
@@ -121,6 +145,8 @@ static __device__ void herm_eigh(cd *A, int lda, cd *V, int ldv, int n, double *
         }
         __syncthreads();
       }
+      if (!rotated_sh) break;
+      __syncthreads();
     }
   }
   for (int i = tid; i < n; i += nt) w[i] = A[i * lda + i].x;
@@ -315,6 +341,171 @@ static __device__ void apply_q(const cd *A, int M, int kk, const cd *tau, cd *X,
     }
     __syncthreads();
   }
+}
+
+// ------------------------------------------------------------------ warp
+// Warp-synchronous forms for small matrices (n <= 32): one warp owns a
+// matrix in its own shared memory, so phases are separated by __syncwarp
+// only and many matrices proceed per SM at once. Same Hermitisation,
+// rotations, pair schedule and stopping rules as the CTA forms above.
+
+// Hermitian eigendecomposition (herm_eigh). V may be null (eigenvalues only).
+// rots: >= n/2+1 entries of the warp's shared memory.
+static __device__ void warp_herm_eigh(cd *A, int lda, cd *V, int ldv, int n, double *w, Rot *rots,
+                                      int max_sweeps = 40) {
+  const int lane = threadIdx.x & 31;
+  if (V)
+    for (int i = lane; i < n * n; i += 32) V[(i / n) * ldv + (i % n)] = (i / n == i % n) ? mk(1.0, 0.0) : czero();
+  for (int i = lane; i < n * n; i += 32) {
+    const int r = i / n, c = i % n;
+    if (r < c) {
+      const cd u = A[r * lda + c], l = A[c * lda + r];
+      const cd h = mk(0.5 * (u.x + l.x), 0.5 * (u.y - l.y));
+      A[r * lda + c] = h;
+      A[c * lda + r] = cconj(h);
+    } else if (r == c) {
+      A[r * lda + c].y = 0.0;
+    }
+  }
+  __syncwarp();
+  const int np = n + (n & 1);
+  const int npairs = np / 2;
+  if (n > 1) {
+    for (int sweep = 0; sweep < max_sweeps; ++sweep) {
+      double off = 0.0, dia = 0.0;
+      for (int i = lane; i < n * n; i += 32) {
+        int r = i / n, c = i % n;
+        double v = cabs2(A[r * lda + c]);
+        if (r == c)
+          dia += v;
+        else if (r < c)
+          off += 2.0 * v;
+      }
+      off = warp_sum(off);
+      dia = warp_sum(dia);
+      if (off == 0.0 || off <= 1e-30 * dia) break;
+      bool rotated = false;
+      for (int step = 0; step < np - 1; ++step) {
+        if (lane < npairs) {
+          int p, q;
+          rr_pair(step, lane, np, p, q);
+          Rot r;
+          r.p = -1;
+          r.q = q;
+          if (q < n) {
+            double a = A[p * lda + p].x, b = A[q * lda + q].x;
+            cd c = A[p * lda + q];
+            double ac2 = cabs2(c);
+            if (ac2 > 0.0 && ac2 >= 1e-36 * (a * a + b * b) && jacobi_rot(a, b, c, r)) {
+              r.p = p;
+              rotated = true;
+            }
+          }
+          rots[lane] = r;
+        }
+        __syncwarp();
+        for (int idx = lane; idx < npairs * n; idx += 32) {
+          const Rot &r = rots[idx / n];
+          if (r.p < 0) continue;
+          int row = idx % n;
+          cd x = A[row * lda + r.p], y = A[row * lda + r.q];
+          A[row * lda + r.p] = cadd(cmul(x, r.j00), cmul(y, r.j10));
+          A[row * lda + r.q] = cadd(cmul(x, r.j01), cmul(y, r.j11));
+          if (V) {
+            x = V[row * ldv + r.p];
+            y = V[row * ldv + r.q];
+            V[row * ldv + r.p] = cadd(cmul(x, r.j00), cmul(y, r.j10));
+            V[row * ldv + r.q] = cadd(cmul(x, r.j01), cmul(y, r.j11));
+          }
+        }
+        __syncwarp();
+        for (int idx = lane; idx < npairs * n; idx += 32) {
+          const Rot &r = rots[idx / n];
+          if (r.p < 0) continue;
+          int col = idx % n;
+          cd x = A[r.p * lda + col], y = A[r.q * lda + col];
+          A[r.p * lda + col] = cadd(cmulc(r.j00, x), cmulc(r.j10, y));
+          A[r.q * lda + col] = cadd(cmulc(r.j01, x), cmulc(r.j11, y));
+        }
+        __syncwarp();
+      }
+      if (!__any_sync(0xffffffffu, rotated)) break;
+    }
+  }
+  for (int i = lane; i < n; i += 32) w[i] = A[i * lda + i].x;
+  __syncwarp();
+}
+
+// One-sided Jacobi SVD (hestenes) of A (m x n, column-major, lda); lane i
+// rotates pair i of each round-robin step, looping over the rows itself.
+static __device__ void warp_hestenes(cd *A, int lda, int m, int n, cd *V, int ldv, double *s, int max_sweeps = 60) {
+  const int lane = threadIdx.x & 31;
+  for (int i = lane; i < n * n; i += 32) V[(i / n) * ldv + (i % n)] = (i / n == i % n) ? mk(1.0, 0.0) : czero();
+  const double tol = 1.1e-16 * sqrt((double)(m > 1 ? m : 1)) * 2.0;
+  const int np = n + (n & 1);
+  const int npairs = np / 2;
+  __syncwarp();
+  if (n > 1) {
+    for (int sweep = 0; sweep < max_sweeps; ++sweep) {
+      bool rotated = false;
+      for (int step = 0; step < np - 1; ++step) {
+        if (lane < npairs) {
+          int p, q;
+          rr_pair(step, lane, np, p, q);
+          if (q < n) {
+            cd *ap = A + (long long)p * lda, *aq = A + (long long)q * lda;
+            double al = 0.0, be = 0.0;
+            cd ga = czero();
+            for (int r = 0; r < m; ++r) {
+              cd x = ap[r], y = aq[r];
+              al += cabs2(x);
+              be += cabs2(y);
+              cfmac(ga, x, y);
+            }
+            double ag = sqrt(cabs2(ga));
+            Rot rt;
+            if (al > 0.0 && be > 0.0 && ag > tol * sqrt(al) * sqrt(be) && jacobi_rot(al, be, ga, rt)) {
+              rotated = true;
+              for (int k = 0; k < m; ++k) {
+                cd x = ap[k], y = aq[k];
+                ap[k] = cadd(cmul(x, rt.j00), cmul(y, rt.j10));
+                aq[k] = cadd(cmul(x, rt.j01), cmul(y, rt.j11));
+              }
+              cd *vp = V + (long long)p * ldv, *vq = V + (long long)q * ldv;
+              for (int k = 0; k < n; ++k) {
+                cd x = vp[k], y = vq[k];
+                vp[k] = cadd(cmul(x, rt.j00), cmul(y, rt.j10));
+                vq[k] = cadd(cmul(x, rt.j01), cmul(y, rt.j11));
+              }
+            }
+          }
+        }
+        __syncwarp();
+      }
+      if (!__any_sync(0xffffffffu, rotated)) break;
+    }
+  }
+  for (int j = lane; j < n; j += 32) {
+    double t = 0.0;
+    for (int r = 0; r < m; ++r) t += cabs2(A[(long long)j * lda + r]);
+    s[j] = sqrt(t);
+  }
+  __syncwarp();
+}
+
+// perm[j] = index of the j-th largest s (stable), n <= 32, by one warp.
+static __device__ void warp_sort_desc(const double *s, int n, int *perm) {
+  const int lane = threadIdx.x & 31;
+  if (lane < n) {
+    int rank = 0;
+    double sj = s[lane];
+    for (int i = 0; i < n; ++i) {
+      double si = s[i];
+      if (si > sj || (si == sj && i < lane)) ++rank;
+    }
+    perm[rank] = lane;
+  }
+  __syncwarp();
 }
 
 }  // namespace dqz

@@ -96,10 +96,13 @@ class GraphLayout:
         return tuple(self.node_dims(v)) + (int(self.phys[v]),)
 
     def node_sizes(self) -> np.ndarray:
+        """phys * product of the bond dimensions, per node (vectorised over
+        the half-edge table, whose entries are grouped by node)."""
         sizes = np.array(self.phys, dtype=np.int64)
-        for v in range(self.n_nodes):
-            for c in self.node_dims(v):
-                sizes[v] *= c
+        if self.n_halves:
+            dims = self.edge_chi[self.half_edge].astype(np.int64)
+            has = self.degree > 0
+            sizes[has] *= np.multiply.reduceat(dims, self.node_half[has])
         return sizes
 
     def half_chi(self) -> np.ndarray:

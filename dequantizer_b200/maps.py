@@ -282,21 +282,32 @@ def messages_frob_distance(lhs: Dict, rhs: Dict) -> torch.Tensor:
     return out
 
 
-def vidal_gauge_packed(layout: GraphLayout, T, n2e, eps: float):
-    """Vidal gauge on packed arenas: returns (Gamma arena, lambda arena)."""
+def vidal_gauge_packed(layout: GraphLayout, T, n2e, eps: float, out=None, edges=None, nodes=None):
+    """Vidal gauge on packed arenas: returns (Gamma arena, lambda arena).
+
+    ``out`` = (G, lam, orth) arenas to write into (new ones when None);
+    ``edges`` / ``nodes`` (int32 device tensors) restrict the work to those
+    edges (lambdas, orthogonalisers) and nodes (Gamma tensors), leaving the
+    rest of ``out`` as it is."""
     stream = _lib.stream_handle()
     max_chi = layout.max_chi()
-    orth = torch.empty(max(layout.msg_elems, 1), dtype=torch.complex128, device=layout.device)
-    lam = layout.new_lam_arena()
-    nb = _lib.lib().dqz_vidal_edges_scratch_bytes(layout.n_edges, max_chi)
+    if out is None:
+        G = torch.empty_like(T)
+        lam = layout.new_lam_arena()
+        orth = torch.empty(max(layout.msg_elems, 1), dtype=torch.complex128, device=layout.device)
+    else:
+        G, lam, orth = out
+    ne = layout.n_edges if edges is None else int(edges.numel())
+    nb = _lib.lib().dqz_vidal_edges_scratch_bytes(ne, max_chi)
     scratch = _scratch(nb, layout.device) if nb else None
     _lib.call("dqz_vidal_edges", layout.gptr, n2e.data_ptr(), float(eps), orth.data_ptr(), lam.data_ptr(), max_chi,
-              _lib.ptr(scratch), stream)
-    G = torch.empty_like(T)
+              _lib.ptr(edges), ne if edges is not None else 0, _lib.ptr(scratch), stream)
     ms = layout.max_size()
-    nb = _lib.lib().dqz_absorb_scratch_bytes(layout.n_nodes, ms)
+    nn = layout.n_nodes if nodes is None else int(nodes.numel())
+    nb = _lib.lib().dqz_absorb_scratch_bytes(nn, ms)
     scratch = _scratch(nb, layout.device) if nb else None
-    _lib.call("dqz_absorb", layout.gptr, T.data_ptr(), orth.data_ptr(), G.data_ptr(), ms, _lib.ptr(scratch), stream)
+    _lib.call("dqz_absorb", layout.gptr, T.data_ptr(), orth.data_ptr(), G.data_ptr(), ms, _lib.ptr(nodes),
+              nn if nodes is not None else 0, _lib.ptr(scratch), stream)
     return G, lam
 
 
@@ -319,11 +330,23 @@ def get_vidal_gauge_fixing_map(traverser, eps):
     return vidal_gauge_fixing_map
 
 
+def vidal_distance_partial(layout: GraphLayout, G, lam, eps: float, partial=None, halves=None) -> torch.Tensor:
+    """Per-half-edge trace norms (the terms of the Vidal distance) into
+    ``partial`` (float64, one per half-edge; new when None). ``halves`` (int32
+    device tensor) recomputes only those entries."""
+    if partial is None:
+        partial = torch.empty(max(layout.n_halves, 1), dtype=torch.float64, device=layout.device)
+    _lib.call("dqz_vidal_distance", layout.gptr, G.data_ptr(), lam.data_ptr(), float(eps), partial.data_ptr(), None,
+              layout.max_chi(), layout.max_slice(), _lib.ptr(halves), int(halves.numel()) if halves is not None else 0,
+              _lib.stream_handle())
+    return partial
+
+
 def vidal_distance_packed(layout: GraphLayout, G, lam, eps: float) -> torch.Tensor:
     partial = torch.empty(max(layout.n_halves, 1), dtype=torch.float64, device=layout.device)
     out = torch.empty((), dtype=torch.float64, device=layout.device)
     _lib.call("dqz_vidal_distance", layout.gptr, G.data_ptr(), lam.data_ptr(), float(eps), partial.data_ptr(),
-              out.data_ptr(), layout.max_chi(), _lib.stream_handle())
+              out.data_ptr(), layout.max_chi(), layout.max_slice(), None, 0, _lib.stream_handle())
     return out
 
 

@@ -146,20 +146,28 @@ int dqz_repack(const void *src, void *dst, const int64_t *src_off, const int64_t
 
 /* Per edge: eigendecompose both node->edge messages, build sqrt / safe inverse
  * sqrt, SVD of sqrt(m_f) sqrt(m_b)^T; write lambdas and the two
- * orthogonalisers orth[h] (chi x chi, complex128, at half_msg_off[h]). */
+ * orthogonalisers orth[h] (chi x chi, complex128, at half_msg_off[h]).
+ * edges: the n_sel edges to process, or NULL for all; the outputs of the
+ * other edges are left as they are. */
 int dqz_vidal_edges(const dqz_graph_t *g, const void *n2e, double eps, void *orth,
-                    double *lambdas, int32_t max_chi, void *scratch, cudaStream_t stream);
+                    double *lambdas, int32_t max_chi, const int32_t *edges, int32_t n_sel,
+                    void *scratch, cudaStream_t stream);
 size_t dqz_vidal_edges_scratch_bytes(int32_t n_edges, int32_t max_chi);
 /* Per node: T_out = T x_e orth[h_e] over every bond (bond index contracted
- * with the row index), normalised. */
+ * with the row index), normalised. nodes: the n_sel nodes, or NULL for all. */
 int dqz_absorb(const dqz_graph_t *g, const void *tensors_in, const void *orth, void *tensors_out,
-               int32_t max_size, void *scratch, cudaStream_t stream);
+               int32_t max_size, const int32_t *nodes, int32_t n_sel, void *scratch, cudaStream_t stream);
 size_t dqz_absorb_scratch_bytes(int32_t n_nodes, int32_t max_size);
 
-/* ---- Vidal distance (mappings/vidal_distance.py:17-42, tensor_ops.py:143-175) */
+/* ---- Vidal distance (mappings/vidal_distance.py:17-42, tensor_ops.py:143-175)
+ * partial[h] = trace norm for half-edge h; out (optional, NULL to skip) =
+ * sum over all half-edges / (2E). max_slice bounds node size / bond
+ * dimension over the processed half-edges. halves: the n_sel half-edges to
+ * recompute, or NULL for all (the other partial entries are kept). */
 int dqz_vidal_distance(const dqz_graph_t *g, const void *tensors, const double *lambdas,
                        double eps, double *partial /*[2E]*/, double *out,
-                       int32_t max_chi, cudaStream_t stream);
+                       int32_t max_chi, int32_t max_slice, const int32_t *halves, int32_t n_sel,
+                       cudaStream_t stream);
 
 /* ---- Symmetric gauge (mappings/symmetric_gauge.py:17-61, tensor_ops.py:189-199) */
 int dqz_symmetric_gauge(const dqz_graph_t *g, const void *tensors_in, const double *lambdas,

@@ -134,8 +134,13 @@ def test_symmetric_gauge_density_and_lambdas(case):
             assert rel_err(b, a) < TOL
 
 
-def test_vidal_distance_matches_oracle():
-    g = G.get_nd_lattice([3, 2, 2], 2, 3)
+@pytest.mark.parametrize("case", ["small_bonds", "wide_slice", "large_bonds"])
+def test_vidal_distance_matches_oracle(case):
+    """small bonds: one warp per half-edge; a bond slice above 1024 entries
+    (degree 4, chi 12) or bonds above 16 (chi 20): one CTA per half-edge."""
+    g = {"small_bonds": lambda: G.get_nd_lattice([3, 2, 2], 2, 3),
+         "wide_slice": lambda: G.get_nd_lattice([3, 3], 2, 12),
+         "large_bonds": lambda: G.get_random_regular_graph(6, 3, 2, 20, 3)}[case]()
     tensors = random_tensors(g, 9)
     rng = np.random.default_rng(10)
     lambdas = {eid: rng.uniform(0.1, 1, e.dimension) for eid, e in g.edges.items()}
@@ -143,6 +148,73 @@ def test_vidal_distance_matches_oracle():
     a = OM.get_vidal_gauge_distance_map(trav, 1e-10)(tensors, lambdas)
     b = float(M.get_vidal_gauge_distance_map(trav, 1e-10)(tensors, lambdas))
     assert abs(a - b) < 1e-10 * max(1.0, a)
+
+
+def test_vidal_gauge_large_bonds_matches_oracle():
+    """chi 20 > 16: the one-CTA-per-edge gauge kernel."""
+    g = G.get_random_regular_graph(6, 3, 2, 20, 3)
+    tensors = random_tensors(g, 4)
+    trav, msgs = _converged_messages(g, tensors, n=60, tol=1e-12)
+    eps = 1e-10
+    r_t, r_l = OM.get_vidal_gauge_fixing_map(trav, eps)(tensors, msgs)
+    g_t, g_l = M.get_vidal_gauge_fixing_map(trav, eps)(tensors, msgs)
+    for eid in r_l:
+        assert rel_err(g_l[eid], r_l[eid]) < TOL_SVD
+    for nid in r_t:
+        assert abs(np.linalg.norm(to_np(g_t[nid])) - 1.0) < 1e-12
+    # Gamma is fixed up to singular-vector phases: compare the gauge-invariant
+    # Vidal distance of both gauges, each measured by the oracle
+    vd = OM.get_vidal_gauge_distance_map(trav, eps)
+    vd_gpu = vd({k: to_np(v) for k, v in g_t.items()}, {k: to_np(v) for k, v in g_l.items()})
+    assert abs(vd_gpu - vd(r_t, r_l)) < 1e-9
+
+
+def test_gauge_selection_updates_only_listed_entries():
+    """vidal_edges / absorb / vidal_distance with index lists: the listed
+    edges, nodes and half-edges equal a full pass, the rest keep their
+    previous contents."""
+    from dequantizer_b200.layout import GraphLayout
+
+    g = G.get_random_regular_graph(12, 3, 2, 4, 2)
+    tensors = random_tensors(g, 5)
+    trav, msgs = _converged_messages(g, tensors, n=30)
+    topo = M.Topology(trav, True)
+    L = GraphLayout(topo.nodes, topo.edges, [e.dimension for e in topo.edges])
+    T = L.pack_tensors([torch.from_numpy(tensors[n.id]).cuda() for n in topo.nodes])
+    n2e = L.pack_messages([torch.from_numpy(msgs[MessageID(nd.id, e.id)]).cuda() for nd, e in topo.half_ids()])
+    G_full, lam_full = M.vidal_gauge_packed(L, T, n2e, 1e-10)
+    part_full = M.vidal_distance_partial(L, G_full, lam_full, 1e-10)
+    rng = np.random.default_rng(0)
+    edges = np.sort(rng.choice(L.n_edges, L.n_edges // 3, replace=False)).astype(np.int32)
+    nodes = np.sort(rng.choice(L.n_nodes, L.n_nodes // 2, replace=False)).astype(np.int32)
+    halves = np.sort(rng.choice(L.n_halves, L.n_halves // 4, replace=False)).astype(np.int32)
+    Gm = torch.full_like(G_full, 7.0)
+    lam = torch.full_like(lam_full, 7.0)
+    orth = torch.full((max(L.msg_elems, 1),), 7.0, dtype=torch.complex128, device=T.device)
+    M.vidal_gauge_packed(L, T, n2e, 1e-10, out=(Gm, lam, orth), edges=torch.from_numpy(edges).cuda())
+    for e in range(L.n_edges):
+        o, c = int(L.edge_lam_off[e]), int(L.edge_chi[e])
+        if e in edges:
+            assert torch.equal(lam[o:o + c], lam_full[o:o + c])
+        else:
+            assert bool((lam[o:o + c] == 7.0).all())
+    # absorb over the listed nodes with every orthogonaliser in place
+    M.vidal_gauge_packed(L, T, n2e, 1e-10, out=(Gm, lam, orth))
+    G2 = torch.full_like(G_full, 7.0)
+    M.vidal_gauge_packed(L, T, n2e, 1e-10, out=(G2, lam, orth), nodes=torch.from_numpy(nodes).cuda())
+    for v in range(L.n_nodes):
+        o, n = int(L.node_off[v]), int(L.node_sizes()[v])
+        if v in nodes:
+            assert torch.equal(G2[o:o + n], G_full[o:o + n])
+        else:
+            assert bool((G2[o:o + n] == 7.0).all())
+    part = torch.full_like(part_full, -1.0)
+    M.vidal_distance_partial(L, G_full, lam_full, 1e-10, part, halves=torch.from_numpy(halves).cuda())
+    mask = np.zeros(L.n_halves, dtype=bool)
+    mask[halves] = True
+    p, q = part.cpu().numpy(), part_full.cpu().numpy()
+    assert np.array_equal(p[mask], q[mask])
+    assert np.all(p[~mask] == -1.0)
 
 
 def test_apply1_apply2_match_oracle():

@@ -106,3 +106,22 @@ def test_annealing_matches_oracle(second_order):
     assert np.abs(res.vidal_distances_after_regauging - np.array(em.after_regauging_vidal_distances)).max() < 1e-9
     spins = 2 * (res.density_matrices[:, 0, 0].real > 0.5) - 1
     assert np.isfinite(W.eval_energy(energy, spins))
+
+
+def test_batched_annealer_equals_independent_runs():
+    """Instances advanced together (one launch per operation over all of
+    them) give the same density matrices and truncation errors as separate
+    runs of the emulator loop (synchronous BP schedule on both sides)."""
+    from dequantizer_b200.annealing import BatchedAnnealer
+
+    energies = [W.random_regular_energy(n, 3, seed=10 + n, field_std=0.5) for n in (8, 10, 12)]
+    steps = list(W.scheduler(0.2, lambda t: 1 - t, 5))
+    ba = BatchedAnnealer(energies, max_chi=4, accuracy=1e-8, max_belief_propagation_iterations=100)
+    rho_b = ba.run(steps)
+    errs_b = ba.truncation_errors()
+    for k, en in enumerate(energies):
+        res = W.run_quantum_annealer(en, steps, key=1, max_chi=4, gates_number_per_regauging=en.edges_number,
+                                     accuracy=1e-8, max_belief_propagation_iterations=100,
+                                     synchronous_update=True)
+        assert np.abs(rho_b[k] - res.density_matrices).max() < 1e-9
+        assert np.abs(errs_b[k] - res.truncation_errors).max() < 1e-9

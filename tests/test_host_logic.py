@@ -70,6 +70,51 @@ def test_decompose_gates_matches_oracle(seed):
     assert flat.shape == (7, 2, 4 * _lib.MAX_PHYS**2) and (ranks == 4).all()
 
 
+def _diag_cases(rng):
+    n = 400
+    J = rng.choice([-1.0, 1.0], n)
+    h1, h2 = rng.normal(size=n), rng.normal(size=n)
+    s1, s2 = np.array([1.0, 1.0, -1.0, -1.0]), np.array([1.0, -1.0, 1.0, -1.0])
+    ham = J[:, None] * s1 * s2 + h1[:, None] * s1 + h2[:, None] * s2
+    out = [np.exp(-1j * tau * ham) for tau in (0.0, 1e-12, 0.05, 0.7, np.pi / 4, np.pi / 2)]
+    out.append(rng.standard_normal((n, 4)) + 1j * rng.standard_normal((n, 4)))  # generic complex
+    z = rng.standard_normal((n, 4)) + 1j * rng.standard_normal((n, 4))
+    z[: n // 4, 0] = 0.0  # zero entries
+    z[n // 4 : n // 2, :2] = 0.0  # zero row
+    z[n // 2 : 3 * n // 4, 1] = z[n // 2 : 3 * n // 4, 0]  # rank one: rows equal
+    z[n // 2 : 3 * n // 4, 3] = z[n // 2 : 3 * n // 4, 2]
+    out.append(z)
+    out.append(np.zeros((3, 4), dtype=np.complex128))
+    return out
+
+
+@pytest.mark.parametrize("seed", range(3))
+def test_diagonal_gate_split_matches_dense_split(seed):
+    """Closed-form split of diagonal gates: same ranks as the dense SVD split,
+    and the halves contract to the same (rank-truncated) gate, within 1e-14."""
+    from dequantizer_b200.gates import decompose_diagonal_gates, expand_diagonal_halves
+
+    for diag in _diag_cases(np.random.default_rng(seed)):
+        n = diag.shape[0]
+        gates = np.zeros((n, 4, 4), dtype=np.complex128)
+        gates[:, np.arange(4), np.arange(4)] = diag
+        gates = gates.reshape(n, 2, 2, 2, 2)
+        dense, r_dense, _ = decompose_gates(gates, 1e-10)
+        compact, ranks = decompose_diagonal_gates(diag, 1e-10)
+        assert (ranks == r_dense).all()
+
+        def contract(flat):
+            h1 = flat[:, 0, :16].reshape(n, 4, 2, 2)
+            h2 = flat[:, 1, :16].reshape(n, 4, 2, 2)
+            return np.einsum("nrai,nrbj->nabij", h1, h2)
+
+        # equal to the dense split's product (which drops singular values <= eps too)
+        back = contract(expand_diagonal_halves(compact))
+        assert np.abs(back - contract(dense)).max() < 1e-14 * max(1.0, np.abs(diag).max())
+        # discarded ranks are zero
+        assert np.all(compact[ranks < 2][:, :, 2:] == 0)
+
+
 @pytest.mark.parametrize("seed", range(6))
 def test_simple_update_shape_rule_matches_oracle(seed):
     rng = np.random.default_rng(seed)
