@@ -100,16 +100,19 @@ __device__ __forceinline__ void load_shape(const dqz_graph_t &g, int v, NodeShap
 // Generic CTA-cooperative mode product on a row-major tensor:
 //   Y[l, i, r] = sum_b M(i, b) X[l, b, r],  M(i, b) = m[i * rs + b * cs] (optionally conj)
 // X has shape (L, qin, R); Y has shape (L, qout, R). X and Y must not alias.
-template <bool CONJ>
-__device__ __forceinline__ void mode_product(const cd *__restrict__ X, cd *__restrict__ Y, long long L, int qin,
-                                             int qout, long long R, const cd *__restrict__ m, int rs, int cs) {
-  const long long total = L * qout * R;
-  for (long long o = threadIdx.x; o < total; o += blockDim.x) {
-    long long r = o % R;
-    long long t = o / R;
-    int i = (int)(t % qout);
-    long long l = t / qout;
-    const cd *x = X + (l * qin) * R + r;
+// Index arithmetic is 32-bit when both tensors have fewer than 2^31 entries
+// (always so for shared-memory operands); 64-bit division is a long
+// instruction sequence and otherwise dominates these small contractions.
+template <bool CONJ, typename I>
+__device__ __forceinline__ void mode_product_idx(const cd *__restrict__ X, cd *__restrict__ Y, I L, int qin,
+                                                 int qout, I R, const cd *__restrict__ m, int rs, int cs) {
+  const I total = L * (I)qout * R;
+  for (I o = threadIdx.x; o < total; o += blockDim.x) {
+    I r = o % R;
+    I t = o / R;
+    int i = (int)(t % (I)qout);
+    I l = t / (I)qout;
+    const cd *x = X + (long long)(l * (I)qin) * R + r;
     const cd *mm = m + (long long)i * rs;
     cd acc = czero();
     for (int b = 0; b < qin; ++b) {
@@ -119,6 +122,16 @@ __device__ __forceinline__ void mode_product(const cd *__restrict__ X, cd *__res
     }
     Y[o] = acc;
   }
+}
+
+template <bool CONJ>
+__device__ __forceinline__ void mode_product(const cd *__restrict__ X, cd *__restrict__ Y, long long L, int qin,
+                                             int qout, long long R, const cd *__restrict__ m, int rs, int cs) {
+  const long long big = (qin > qout ? qin : qout);
+  if (L * big * R < (1ll << 31))
+    mode_product_idx<CONJ, int>(X, Y, (int)L, qin, qout, (int)R, m, rs, cs);
+  else
+    mode_product_idx<CONJ, long long>(X, Y, L, qin, qout, R, m, rs, cs);
 }
 
 }  // namespace dqz

@@ -157,6 +157,14 @@ static __device__ void herm_eigh(cd *A, int lda, cd *V, int ldv, int n, double *
 // is not required but only min(m, n) columns come out non-zero when m < n.
 // On return column j of A is s_j u_j, V (n x n, column-major, ldv) holds the
 // right singular vectors, s[j] = |A_j| (unsorted). One warp rotates a pair.
+// Columns whose squared norm falls to (m eps)^2 ||A||_F^2 are numerically
+// null: they take part in no rotation (their mutual orthogonality is rounding
+// noise and never settles) and are returned with s[j] = 0.
+__host__ __device__ inline double hestenes_null_scale(int m) {
+  const double t = (double)(m > 1 ? m : 1) * 2.220446049250313e-16;
+  return t * t;
+}
+
 static __device__ void hestenes(cd *A, int lda, int m, int n, cd *V, int ldv, double *s, int *flag, double *red,
                          int max_sweeps = 60) {
   const int tid = threadIdx.x, nt = blockDim.x;
@@ -165,7 +173,9 @@ static __device__ void hestenes(cd *A, int lda, int m, int n, cd *V, int ldv, do
   const double tol = 1.1e-16 * sqrt((double)(m > 1 ? m : 1)) * 2.0;
   const int np = n + (n & 1);
   const int npairs = np / 2;
-  __syncthreads();
+  double fro = 0.0;
+  for (int i = tid; i < m * n; i += nt) fro += cabs2(A[(long long)(i / m) * lda + (i % m)]);
+  const double null_thr = hestenes_null_scale(m) * block_sum(fro, red);
   if (n > 1) {
     for (int sweep = 0; sweep < max_sweeps; ++sweep) {
       if (tid == 0) *flag = 0;
@@ -188,7 +198,7 @@ static __device__ void hestenes(cd *A, int lda, int m, int n, cd *V, int ldv, do
           be = warp_sum(be);
           ga = warp_csum(ga);
           double ag = sqrt(cabs2(ga));
-          if (!(al > 0.0) || !(be > 0.0) || !(ag > tol * sqrt(al) * sqrt(be))) continue;
+          if (!(al > null_thr) || !(be > null_thr) || !(ag > tol * sqrt(al) * sqrt(be))) continue;
           Rot r;
           if (!jacobi_rot(al, be, ga, r)) continue;
           if (lane == 0) *flag = 1;
@@ -214,7 +224,7 @@ static __device__ void hestenes(cd *A, int lda, int m, int n, cd *V, int ldv, do
     double t = 0.0;
     for (int r = lane; r < m; r += 32) t += cabs2(A[(long long)j * lda + r]);
     t = warp_sum(t);
-    if (lane == 0) s[j] = sqrt(t);
+    if (lane == 0) s[j] = t > null_thr ? sqrt(t) : 0.0;
   }
   __syncthreads();
 }
@@ -438,12 +448,16 @@ static __device__ void warp_herm_eigh(cd *A, int lda, cd *V, int ldv, int n, dou
 
 // One-sided Jacobi SVD (hestenes) of A (m x n, column-major, lda); lane i
 // rotates pair i of each round-robin step, looping over the rows itself.
+// Same null-column rule as hestenes.
 static __device__ void warp_hestenes(cd *A, int lda, int m, int n, cd *V, int ldv, double *s, int max_sweeps = 60) {
   const int lane = threadIdx.x & 31;
   for (int i = lane; i < n * n; i += 32) V[(i / n) * ldv + (i % n)] = (i / n == i % n) ? mk(1.0, 0.0) : czero();
   const double tol = 1.1e-16 * sqrt((double)(m > 1 ? m : 1)) * 2.0;
   const int np = n + (n & 1);
   const int npairs = np / 2;
+  double fro = 0.0;
+  for (int i = lane; i < m * n; i += 32) fro += cabs2(A[(long long)(i / m) * lda + (i % m)]);
+  const double null_thr = hestenes_null_scale(m) * warp_sum(fro);
   __syncwarp();
   if (n > 1) {
     for (int sweep = 0; sweep < max_sweeps; ++sweep) {
@@ -464,7 +478,7 @@ static __device__ void warp_hestenes(cd *A, int lda, int m, int n, cd *V, int ld
             }
             double ag = sqrt(cabs2(ga));
             Rot rt;
-            if (al > 0.0 && be > 0.0 && ag > tol * sqrt(al) * sqrt(be) && jacobi_rot(al, be, ga, rt)) {
+            if (al > null_thr && be > null_thr && ag > tol * sqrt(al) * sqrt(be) && jacobi_rot(al, be, ga, rt)) {
               rotated = true;
               for (int k = 0; k < m; ++k) {
                 cd x = ap[k], y = aq[k];
@@ -488,7 +502,7 @@ static __device__ void warp_hestenes(cd *A, int lda, int m, int n, cd *V, int ld
   for (int j = lane; j < n; j += 32) {
     double t = 0.0;
     for (int r = 0; r < m; ++r) t += cabs2(A[(long long)j * lda + r]);
-    s[j] = sqrt(t);
+    s[j] = t > null_thr ? sqrt(t) : 0.0;
   }
   __syncwarp();
 }
