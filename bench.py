@@ -226,7 +226,13 @@ def measure_peak(torch, dtype):
 # DRAM bytes (read + write) per node-update launch from one ncu capture of
 # the bench workload; profiles/ holds the summaries these come from.
 NCU_TRAFFIC = {
+    # dram__bytes_read.sum + dram__bytes_write.sum per launch, from the ncu
+    # captures summarised under profiles/ (same workload: 1024-node 3-regular
+    # graph, chi 16, one launch over all 3072 half-edges)
     ("bp_node_generic", "fp64"): 166.6e6,
+    ("bp_node_k3", "fp64"): 158.0e6,
+    ("bp_node_k3", "fp32"): 77.6e6,
+    ("bp_node_k3_tc", "bf16"): 39.9e6,
 }
 
 

@@ -86,6 +86,8 @@ _SIGNATURES = {
     "dqz_messages_distance": (ctypes.c_int, [_G, _P, _P, _P, _P, _P, _P, _I, _P]),
     "dqz_reduce_sum": (ctypes.c_int, [_P, _I, _D, _P, _P]),
     "dqz_segment_distance": (ctypes.c_int, [_P, _P, _P, _I, _P, _P, _P]),
+    "dqz_bp_node_vjp": (ctypes.c_int, [_G, _P, _P, _P, _P, _P, _P, _I, _I, _I, _P, _P]),
+    "dqz_bp_node_vjp_scratch_bytes": (_S, [_I, _I]),
     "dqz_vidal_edges": (ctypes.c_int, [_G, _P, _D, _P, _P, _I, _P, _I, _P, _P]),
     "dqz_vidal_edges_scratch_bytes": (_S, [_I, _I]),
     "dqz_absorb": (ctypes.c_int, [_G, _P, _P, _P, _I, _P, _I, _P, _P]),

@@ -142,6 +142,19 @@ int dqz_segment_distance(const void *a, const void *b, const int64_t *seg_off, i
 int dqz_repack(const void *src, void *dst, const int64_t *src_off, const int64_t *dst_off,
                const int64_t *count, int32_t n, int32_t elem_bytes, cudaStream_t stream);
 
+/* ---- Adjoint of the node update (reverse of tensor_ops.py:36-60) ----------
+ * Transposed message sweep for implicit differentiation at a BP fixed point.
+ * For each listed node v and each bond e, with n2e_cot[(v,e)] the cotangent
+ * of the outgoing message N_{v,e}(T_v, {e2n[(v,f)]}_{f != e}):
+ *   e2n_cot[(v,f)] = sum_{e != f} (dN_{v,e} / d e2n[(v,f)])^* n2e_cot[(v,e)]
+ *   t_cot[v]      += sum_e (dN_{v,e} / dT_v)^* n2e_cot[(v,e)]   (t_cot may be NULL)
+ * Cotangents are grad z = dL/dRe z + i dL/dIm z. e2n_cot entries of the listed
+ * nodes are overwritten; max_size / max_chi bound the node sizes and bonds. */
+int dqz_bp_node_vjp(const dqz_graph_t *g, const void *tensors, const void *e2n, const void *n2e_cot,
+                    void *e2n_cot, void *t_cot, const int32_t *nodes, int32_t n_nodes, int32_t max_size,
+                    int32_t max_chi, void *scratch, cudaStream_t stream);
+size_t dqz_bp_node_vjp_scratch_bytes(int32_t n_nodes, int32_t max_size);
+
 /* ---- Vidal gauge (mappings/vidal_gauge.py:21-63, tensor_ops.py:88-130) ---- */
 
 /* Per edge: eigendecompose both node->edge messages, build sqrt / safe inverse
