@@ -37,18 +37,26 @@ class FixedPointProblem:
     """Packed layout and flooding-sweep tables of one tensor graph, plus the
     scratch of the transposed sweep. Bond dimensions are those of the graph."""
 
-    def __init__(self, graph: TensorGraph, traversal: str = "dfs"):
+    def __init__(self, graph: TensorGraph, traversal: str = "dfs", topo: Optional[Topology] = None):
+        """``topo``: a flooding Topology of the same graph to reuse (its
+        traversal fixes node and edge order); bond dimensions are read from
+        the graph's edges either way."""
         if not torch.cuda.is_available():
             raise RuntimeError("the adjoint runs on the GPU only")
         _lib.lib()
-        trav = list(graph.get_traversal_iterator(ordering=traversal))
-        self.topo = Topology(trav, True, flooding=True)
+        if topo is None:
+            trav = list(graph.get_traversal_iterator(ordering=traversal))
+            topo = Topology(trav, True, flooding=True)
+        elif not topo.flooding:
+            raise ValueError("the fixed-point problem needs a flooding topology")
+        self.topo = topo
         self.layout = GraphLayout(self.topo.nodes, self.topo.edges, [e.dimension for e in self.topo.edges])
         L = self.layout
         self.nodes_dev = torch.arange(L.n_nodes, dtype=torch.int32, device=L.device)
         self._edge_all = torch.ones(max(L.n_halves, 1), dtype=torch.uint8, device=L.device)
-        nb = _lib.lib().dqz_bp_node_vjp_scratch_bytes(L.n_nodes, L.max_size())
-        self._scratch = torch.empty(max(int(nb), 1), dtype=torch.uint8, device=L.device)
+        self._scratch = None
+        self.last_sweeps = 0
+        self.last_adjoint_sweeps = 0
 
     # ------------------------------------------------------------ plumbing
     def swap(self, src: torch.Tensor) -> torch.Tensor:
@@ -74,13 +82,18 @@ class FixedPointProblem:
             d = float((n2e_new - n2e).abs().max())
             n2e, e2n = n2e_new, e2n_new
             if d <= tol:
+                self.last_sweeps = it
                 return n2e, e2n, it
+        self.last_sweeps = max_sweeps
         return n2e, e2n, max_sweeps
 
     def node_vjp(self, T, e2n, n2e_cot, t_cot: Optional[torch.Tensor] = None) -> torch.Tensor:
         """Transposed node update: returns the e2n cotangent arena; adds the
         node-tensor cotangent into t_cot when given."""
         L = self.layout
+        if self._scratch is None:
+            nb = _lib.lib().dqz_bp_node_vjp_scratch_bytes(L.n_nodes, L.max_size())
+            self._scratch = torch.empty(max(int(nb), 1), dtype=torch.uint8, device=L.device)
         out = torch.zeros_like(e2n)
         _lib.call("dqz_bp_node_vjp", L.gptr, T.data_ptr(), e2n.data_ptr(), n2e_cot.data_ptr(), out.data_ptr(),
                   _lib.ptr(t_cot), self.nodes_dev.data_ptr(), L.n_nodes, L.max_size(), L.max_chi(),
@@ -116,11 +129,10 @@ class BPFixedPoint(torch.autograd.Function):
     def forward(ctx, T, problem: FixedPointProblem, n2e0, tol: float = 1e-13, max_sweeps: int = 1000,
                 adj_tol: float = 1e-13, adj_max: int = 1000):
         T = T.detach()
-        n2e, e2n, sweeps = problem.converge(T, n2e0.detach(), tol, max_sweeps)
+        n2e, e2n, _ = problem.converge(T, n2e0.detach(), tol, max_sweeps)
         ctx.problem = problem
         ctx.adj_tol, ctx.adj_max = adj_tol, adj_max
         ctx.save_for_backward(T, n2e, e2n)
-        problem.last_sweeps = sweeps
         return n2e, e2n
 
     @staticmethod

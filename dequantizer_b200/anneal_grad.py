@@ -1,0 +1,361 @@
+"""Gradient of the final annealing energy with respect to the per-step
+schedule values s_t, by a hand-written reverse pass with checkpointing.
+
+Forward (one instance, Vidal form (Gamma, lambda), FP64 complex128):
+  |+> product state; for t = 0..N-1 (second-order Trotter step of
+  H(s) = -(1 - s) sum X + s sum J Z Z, dt fixed):
+    regauge (t > 0): symmetric gauge (tensor_ops.py:189-199), BP to its fixed
+        point from lambda messages (``BPFixedPoint``: CUDA sweeps forward,
+        implicit adjoint with the transposed-sweep kernel backward), Vidal
+        gauge (tensor_ops.py:88-130: eigh, square roots, SVD, absorb);
+    exp(-i tau_m/2 X) on every qubit (tensor_graph.py:268-275);
+    exp(-i tau_c (J Z Z + h_u/deg_u Z + h_v/deg_v Z)) on every coupled pair,
+        in pair order, by simple update truncated to max_chi
+        (tensor_ops.py:265-389);
+    exp(-i tau_m/2 X) on every qubit;
+  with tau_m = -dt (1 - s_t), tau_c = dt s_t; then a final regauge and
+  E = sum_e J_e <Z_u Z_v> from the two-site reduced density matrices of the
+  Vidal form.
+
+Differences from the reference loop that keep the map smooth in s:
+  * BP runs to its fixed point (max message change <= ``bp_tol``) instead of
+    stopping at a Vidal-distance threshold, so the regauge is a function of
+    the state;
+  * a coupling gate is split analytically into two rank-2 halves,
+    h1 = (cos(tau J) e^{-i tau h_u z}, -i sin(tau J) z e^{-i tau h_u z}),
+    h2 = (e^{-i tau h_v z}, z e^{-i tau h_v z}), instead of by SVD; the product
+    h1 . h2 is the same gate, so the physical state is unchanged (only the
+    representation's scale factors differ);
+  * the truncated two-site decomposition is the SVD of
+    Theta = A_u diag(lambda_e x 1_r) A_v^T through ``product_svd`` (the
+    reference's QR + core SVD forward, with the adjoint of Theta's own SVD).
+Reverse pass: the forward stores (Gamma, lambda) every ``checkpoint_every``
+steps; segments are recomputed under autograd in reverse order and
+differentiated with the hand-written SVD / eigh adjoints of ``linalg_ad`` and
+the implicit BP adjoint.
+"""
+
+import math
+from typing import Dict, List, Sequence, Tuple
+
+import numpy as np
+import torch
+
+from .adjoint import BPFixedPoint, FixedPointProblem
+from .graph import TensorGraph
+from .linalg_ad import eigh, product_svd, svd
+from .maps import Topology
+from .workloads import EnergyFunction, tensor_graph_of
+
+F32_MAX = 3.4028234663852886e38
+EPS = 1e-10
+
+
+def safe_inverse(x: torch.Tensor, eps: float) -> torch.Tensor:
+    """tensor_ops.py:20-21."""
+    return 1.0 / ((x < eps).to(x.dtype) * F32_MAX + x)
+
+
+def safe_sqrt_truncate(x: torch.Tensor, eps: float) -> torch.Tensor:
+    """sqrt(safe_truncate(x)) with a finite derivative at the truncated entries."""
+    keep = x > eps
+    return torch.where(keep, torch.sqrt(torch.where(keep, x, torch.ones_like(x))), torch.zeros_like(x))
+
+
+def _bcast(vec: torch.Tensor, axis: int, ndim: int) -> torch.Tensor:
+    shape = [1] * ndim
+    shape[axis] = vec.shape[0]
+    return vec.reshape(shape)
+
+
+class AnnealingGradient:
+    """Differentiable annealing of one instance on the GPU."""
+
+    def __init__(self, energy: EnergyFunction, max_chi: int, dt: float, checkpoint_every: int = 10,
+                 bp_tol: float = 1e-13, bp_max: int = 2000, eps: float = EPS, device=None):
+        if not torch.cuda.is_available():
+            raise RuntimeError("the annealing gradient runs on the GPU only")
+        self.energy = energy
+        self.max_chi = int(max_chi)
+        self.dt = float(dt)
+        self.k = int(checkpoint_every)
+        self.bp_tol, self.bp_max, self.eps = bp_tol, bp_max, eps
+        self.device = device or torch.device("cuda", torch.cuda.current_device())
+        self.graph: TensorGraph = tensor_graph_of(energy)
+        self.trav = list(self.graph.get_traversal_iterator())
+        self.topo = Topology(self.trav, True, flooding=True)
+        self.nodes = self.topo.nodes
+        self.edges = self.topo.edges
+        self.node_idx = {n.id: i for i, n in enumerate(self.nodes)}
+        self.edge_idx = {e.id: i for i, e in enumerate(self.edges)}
+        self.node_edges = [[self.edge_idx[e.id] for e in n.neighbors] for n in self.nodes]
+        # edge -> (node a, bond index at a, node b, bond index at b), a = neighbours[0]
+        self.edge_ends = []
+        for e in self.edges:
+            a, b = e.neighbors[0], e.neighbors[1]
+            self.edge_ends.append((self.node_idx[a.id], a.indices[e.id], self.node_idx[b.id], b.indices[e.id]))
+        deg = {n.id: len(n.neighbors) for n in self.nodes}
+        self.gates = []  # (edge, node1, bond1, node2, bond2, J, h1/deg1, h2/deg2) in pair order
+        for (a, b), J in zip(energy.coupled_spin_pairs, energy.coupling_amplitudes):
+            a, b = int(a), int(b)
+            e = self.graph.find_edge(a, b)
+            na, nb = self.graph.get_node(a), self.graph.get_node(b)
+            self.gates.append((self.edge_idx[e.id], self.node_idx[a], na.indices[e.id], self.node_idx[b],
+                               nb.indices[e.id], float(J), float(energy.fields[a]) / deg[a],
+                               float(energy.fields[b]) / deg[b]))
+        self.z = torch.tensor([1.0, -1.0], dtype=torch.float64, device=self.device)
+        self.last_bp_sweeps: List[int] = []
+
+    # ------------------------------------------------------------- state
+    def initial_state(self) -> Tuple[List[torch.Tensor], List[torch.Tensor]]:
+        """|+> on every qubit, all bonds of dimension 1, lambda = 1."""
+        plus = torch.full((2,), math.sqrt(0.5), dtype=torch.complex128, device=self.device)
+        gam = [plus.reshape((1,) * len(n.neighbors) + (2,)).clone() for n in self.nodes]
+        lam = [torch.ones(1, dtype=torch.float64, device=self.device) for _ in self.edges]
+        return gam, lam
+
+    # ---------------------------------------------------------- gates
+    def mixing_gate(self, tau):
+        """exp(-i tau X) (quantum_annealer.py:72-84)."""
+        c, s = torch.cos(tau), torch.sin(tau)
+        zero = torch.zeros_like(c)
+        re = torch.stack([torch.stack([c, zero]), torch.stack([zero, c])])
+        im = torch.stack([torch.stack([zero, -s]), torch.stack([-s, zero])])
+        return torch.complex(re, im)
+
+    def coupling_halves(self, tau, J: float, hu: float, hv: float):
+        """Rank-2 halves (r, o, i) of exp(-i tau (J ZZ + hu Z + hv Z)), diagonal in (o, i)."""
+        z = self.z
+        zc = z.to(torch.complex128)
+        pu = torch.exp(torch.complex(torch.zeros_like(z), -tau * hu * z))
+        pv = torch.exp(torch.complex(torch.zeros_like(z), -tau * hv * z))
+        c = torch.cos(tau * J).to(torch.complex128)
+        s = torch.sin(tau * J).to(torch.complex128)
+        h1 = torch.stack([torch.diag(c * pu), torch.diag(-1j * s * zc * pu)])
+        h2 = torch.stack([torch.diag(pv), torch.diag(zc * pv)])
+        return h1, h2
+
+    # ------------------------------------------------------- operations
+    def apply1_all(self, gam, G):
+        out = []
+        for T in gam:
+            t = torch.tensordot(T, G, dims=([T.dim() - 1], [1]))
+            out.append(t / torch.linalg.vector_norm(t))
+        return out
+
+    def _prepare(self, T, lams: Sequence[torch.Tensor], half, index: int):
+        """tensor_ops.py:265-283 up to the QR: lambda-scale the other bonds, apply
+        the half gate (phys contracted with its input, rank merged into bond
+        ``index`` bond-major, normalised), bond ``index`` moved last."""
+        k = T.dim() - 1
+        for f, l in enumerate(lams):
+            if f != index:
+                T = T * _bcast(l.to(T.dtype), f, k + 1)
+        shape = list(T.shape)
+        shape[index] *= half.shape[0]
+        T = torch.tensordot(T, half, dims=([k], [2]))  # (..bonds.., r, o)
+        n = T.dim()
+        T = T.permute(*range(index + 1), n - 2, *range(index + 1, n - 2), n - 1).reshape(shape)
+        T = T / torch.linalg.vector_norm(T)
+        return torch.movedim(T, index, -1)
+
+    def simple_update(self, gam, lam, gate, h1, h2):
+        """tensor_ops.py:318-389 for one gate (rank = min(max_chi, available))."""
+        e, a, ia, b, ib = gate[:5]
+        la = [lam[f] for f in self.node_edges[a]]
+        lb = [lam[f] for f in self.node_edges[b]]
+        Pa = self._prepare(gam[a], la, h1, ia)
+        Pb = self._prepare(gam[b], lb, h2, ib)
+        K = Pa.shape[-1]
+        d = lam[e].repeat_interleave(h1.shape[0]).to(torch.complex128)
+        Wa, S, Wb = product_svd(Pa.reshape(-1, K) * d.unsqueeze(0), Pb.reshape(-1, K))
+        lmbd = (S > self.eps).to(S.dtype) * S
+        rank = min(self.max_chi, S.shape[0])
+
+        def finish(W, P, lams, index):
+            q = W[:, :rank].reshape(P.shape[:-1] + (rank,))
+            nd = q.dim()
+            others = [l for f, l in enumerate(lams) if f != index]
+            for f, l in enumerate(others):
+                q = q * _bcast(safe_inverse(l, self.eps).to(q.dtype), f, nd)
+            return torch.movedim(q, nd - 1, index)  # (others.., phys, rank) -> rank at ``index``
+
+        gam = list(gam)
+        lam = list(lam)
+        gam[a] = finish(Wa, Pa, la, ia)
+        gam[b] = finish(Wb, Pb, lb, ib)
+        lam[e] = lmbd[:rank]
+        return gam, lam
+
+    def coupling_layer(self, gam, lam, tau):
+        for gate in self.gates:
+            h1, h2 = self.coupling_halves(tau, *gate[5:])
+            gam, lam = self.simple_update(gam, lam, gate, h1, h2)
+        return gam, lam
+
+    def _problem(self, lam) -> FixedPointProblem:
+        for e, l in zip(self.edges, lam):
+            e.dimension = int(l.shape[0])
+        return FixedPointProblem(self.graph, topo=self.topo)
+
+    def regauge(self, gam, lam):
+        """Symmetric gauge, BP fixed point, Vidal gauge."""
+        P = self._problem(lam)
+        L = P.layout
+        Ts = []
+        for v, G in enumerate(gam):
+            T = G
+            for f, ei in enumerate(self.node_edges[v]):
+                T = T * _bcast(safe_sqrt_truncate(lam[ei], self.eps).to(T.dtype), f, G.dim())
+            Ts.append(T / torch.linalg.vector_norm(T))
+        T_arena = torch.cat([T.reshape(-1) for T in Ts])
+        with torch.no_grad():
+            n2e0 = torch.zeros(max(L.msg_elems, 1), dtype=torch.complex128, device=self.device)
+            for h in range(L.n_halves):
+                L.message_view(n2e0, h).copy_(torch.diag(lam[int(L.half_edge[h])].to(torch.complex128)))
+        if T_arena.requires_grad:
+            n2e, _ = BPFixedPoint.apply(T_arena, P, n2e0, self.bp_tol, self.bp_max, self.bp_tol, self.bp_max)
+        else:
+            n2e, _, _ = P.converge(T_arena, n2e0, self.bp_tol, self.bp_max)
+        self.last_bp_sweeps.append(P.last_sweeps)
+        msgs = P.messages(n2e)
+        orth: Dict[Tuple[int, int], torch.Tensor] = {}
+        new_lam = []
+        for a, ia, b, ib in self.edge_ends:
+            Gf, Gb, l = self._edge_svd(msgs[int(L.node_half[a]) + ia], msgs[int(L.node_half[b]) + ib])
+            orth[(a, ia)] = Gf
+            orth[(b, ib)] = Gb
+            new_lam.append(l)
+        new_gam = []
+        for v, T in enumerate(Ts):
+            t = T
+            for f in range(T.dim() - 1):
+                t = torch.tensordot(t, orth[(v, f)], dims=([0], [0]))
+            t = t.permute(*range(1, t.dim()), 0)
+            new_gam.append(t / torch.linalg.vector_norm(t))
+        return new_gam, new_lam
+
+    def _edge_svd(self, mf, mb):
+        """tensor_ops.py:108-130."""
+        eps = self.eps
+        lf, uf = eigh(0.5 * (mf + mf.mH))
+        lb, ub = eigh(0.5 * (mb + mb.mH))
+
+        def sq(l, u, inv):
+            w = torch.sqrt(safe_inverse(l, eps)) if inv else safe_sqrt_truncate(l, eps)
+            return (u * w.to(u.dtype).unsqueeze(0)) @ u.mH
+
+        m_sq_inv_f, m_sq_inv_b = sq(lf, uf, True), sq(lb, ub, True)
+        u, s, vh = svd(sq(lf, uf, False) @ sq(lb, ub, False).T)
+        s = s / torch.linalg.vector_norm(s)
+        keep = (s > eps).to(s.dtype)
+        s = keep * s
+        u = u * keep.to(u.dtype).unsqueeze(0)
+        u = u / torch.linalg.vector_norm(u)
+        vh = vh * keep.to(vh.dtype).unsqueeze(1)
+        vh = vh / torch.linalg.vector_norm(vh)
+        return m_sq_inv_f @ u, m_sq_inv_b @ vh.T, s
+
+    def step(self, gam, lam, s_t, first: bool):
+        tau_m = -self.dt * (1.0 - s_t)
+        tau_c = self.dt * s_t
+        if not first:
+            gam, lam = self.regauge(gam, lam)
+        half = self.mixing_gate(tau_m / 2)
+        gam = self.apply1_all(gam, half)
+        gam, lam = self.coupling_layer(gam, lam, tau_c)
+        gam = self.apply1_all(gam, half)
+        return gam, lam
+
+    # ------------------------------------------------------- observables
+    def energy_of(self, gam, lam) -> torch.Tensor:
+        """sum_e J_e <Z_u Z_v> from two-site reduced density matrices of the
+        Vidal form (lambda on every bond of the pair, the shared one once)."""
+        total = torch.zeros((), dtype=torch.float64, device=self.device)
+        zz = self.z.unsqueeze(1) * self.z.unsqueeze(0)
+        for gate in self.gates:
+            e, a, ia, b, ib, J = gate[:6]
+            A = gam[a]
+            for f, ei in enumerate(self.node_edges[a]):
+                A = A * _bcast(lam[ei].to(A.dtype), f, A.dim())
+            B = gam[b]
+            for f, ei in enumerate(self.node_edges[b]):
+                if f != ib:
+                    B = B * _bcast(lam[ei].to(B.dtype), f, B.dim())
+            A = torch.movedim(A, ia, 0)
+            B = torch.movedim(B, ib, 0)
+            theta = torch.tensordot(A, B, dims=([0], [0]))  # (rest_a.., o_a, rest_b.., o_b)
+            theta = torch.movedim(theta, A.dim() - 2, 0)
+            theta = torch.movedim(theta, -1, 1)  # (o_a, o_b, rest..)
+            p = (theta.abs() ** 2).reshape(2, 2, -1).sum(-1)
+            total = total + J * (zz * p).sum() / p.sum()
+        return total
+
+    def one_site_z(self, gam, lam) -> torch.Tensor:
+        """<Z_v> per node (traversal order) from the Vidal form."""
+        out = []
+        for v, G in enumerate(gam):
+            T = G
+            for f, ei in enumerate(self.node_edges[v]):
+                T = T * _bcast(lam[ei].to(T.dtype), f, T.dim())
+            p = (T.abs() ** 2).reshape(-1, 2).sum(0)
+            out.append((p[0] - p[1]) / p.sum())
+        return torch.stack(out)
+
+    # ---------------------------------------------------------- driver
+    def final_state(self, s_values: Sequence[float]):
+        """(Gamma, lambda) after the last step and the final regauge."""
+        s = torch.as_tensor(np.asarray(s_values, dtype=np.float64), device=self.device)
+        gam, lam = self.initial_state()
+        with torch.no_grad():
+            for t in range(s.shape[0]):
+                gam, lam = self.step(gam, lam, s[t], first=(t == 0))
+            return self.regauge(gam, lam)
+
+    def forward(self, s_values: torch.Tensor):
+        """No-grad forward; returns (energy, checkpoints)."""
+        gam, lam = self.initial_state()
+        checkpoints = []
+        with torch.no_grad():
+            for t in range(s_values.shape[0]):
+                if t % self.k == 0:
+                    checkpoints.append((t, [g.clone() for g in gam], [l.clone() for l in lam]))
+                gam, lam = self.step(gam, lam, s_values[t], first=(t == 0))
+            gam, lam = self.regauge(gam, lam)
+            E = self.energy_of(gam, lam)
+        return E, checkpoints
+
+    def energy_value(self, s_values: Sequence[float]) -> float:
+        s = torch.as_tensor(np.asarray(s_values, dtype=np.float64), device=self.device)
+        return float(self.forward(s)[0])
+
+    def value_and_grad(self, s_values: Sequence[float]) -> Tuple[float, np.ndarray]:
+        """E and dE/ds_t for every step, by checkpointed reverse passes."""
+        s_all = torch.as_tensor(np.asarray(s_values, dtype=np.float64), device=self.device)
+        n = s_all.shape[0]
+        E, checkpoints = self.forward(s_all)
+        grad = torch.zeros(n, dtype=torch.float64, device=self.device)
+        cot = None
+        for ci in range(len(checkpoints) - 1, -1, -1):
+            t0, g0, l0 = checkpoints[ci]
+            t1 = checkpoints[ci + 1][0] if ci + 1 < len(checkpoints) else n
+            gam = [g.clone().requires_grad_(True) for g in g0]
+            lam = [l.clone().requires_grad_(True) for l in l0]
+            s_seg = s_all[t0:t1].clone().requires_grad_(True)
+            g_cur, l_cur = gam, lam
+            for j in range(t1 - t0):
+                g_cur, l_cur = self.step(g_cur, l_cur, s_seg[j], first=(t0 + j == 0))
+            if cot is None:
+                g_cur, l_cur = self.regauge(g_cur, l_cur)
+                outs = [self.energy_of(g_cur, l_cur)]
+                gouts = [torch.ones_like(outs[0])]
+            else:
+                pairs = [(o, c) for o, c in zip(list(g_cur) + list(l_cur), cot) if o.requires_grad]
+                outs = [o for o, _ in pairs]
+                gouts = [c for _, c in pairs]
+            ins = list(gam) + list(lam) + [s_seg]
+            grads = torch.autograd.grad(outs, ins, grad_outputs=gouts, allow_unused=True)
+            grads = [torch.zeros_like(x) if gr is None else gr for x, gr in zip(ins, grads)]
+            grad[t0:t1] += grads[-1]
+            cot = grads[:-1]
+        return float(E), grad.cpu().numpy()
