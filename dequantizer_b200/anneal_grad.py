@@ -105,6 +105,17 @@ class AnnealingGradient:
                                float(energy.fields[b]) / deg[b]))
         self.z = torch.tensor([1.0, -1.0], dtype=torch.float64, device=self.device)
         self.last_bp_sweeps: List[int] = []
+        # node-disjoint gate levels in pair order (gates on different nodes act
+        # on different tensors, so a level runs as one batch)
+        last = np.zeros(len(self.nodes), dtype=np.int64)
+        lvl = np.zeros(len(self.gates), dtype=np.int64)
+        for j, gt in enumerate(self.gates):
+            lvl[j] = max(last[gt[1]], last[gt[3]]) + 1
+            last[gt[1]] = last[gt[3]] = lvl[j]
+        self.levels = [np.nonzero(lvl == l)[0].tolist() for l in range(1, int(lvl.max(initial=0)) + 1)]
+        self.gate_J = torch.tensor([g[5] for g in self.gates], dtype=torch.float64, device=self.device)
+        self.gate_hu = torch.tensor([g[6] for g in self.gates], dtype=torch.float64, device=self.device)
+        self.gate_hv = torch.tensor([g[7] for g in self.gates], dtype=torch.float64, device=self.device)
 
     # ------------------------------------------------------------- state
     def initial_state(self) -> Tuple[List[torch.Tensor], List[torch.Tensor]]:
@@ -123,74 +134,117 @@ class AnnealingGradient:
         im = torch.stack([torch.stack([zero, -s]), torch.stack([-s, zero])])
         return torch.complex(re, im)
 
-    def coupling_halves(self, tau, J: float, hu: float, hv: float):
-        """Rank-2 halves (r, o, i) of exp(-i tau (J ZZ + hu Z + hv Z)), diagonal in (o, i)."""
+    def coupling_halves(self, tau, idx: Sequence[int]):
+        """Rank-2 halves (B, r, o, i) of exp(-i tau (J ZZ + hu Z + hv Z)) for the
+        gates ``idx``, diagonal in (o, i)."""
+        ix = torch.as_tensor(idx, device=self.device)
+        J, hu, hv = self.gate_J[ix], self.gate_hu[ix], self.gate_hv[ix]
         z = self.z
         zc = z.to(torch.complex128)
-        pu = torch.exp(torch.complex(torch.zeros_like(z), -tau * hu * z))
-        pv = torch.exp(torch.complex(torch.zeros_like(z), -tau * hv * z))
-        c = torch.cos(tau * J).to(torch.complex128)
-        s = torch.sin(tau * J).to(torch.complex128)
-        h1 = torch.stack([torch.diag(c * pu), torch.diag(-1j * s * zc * pu)])
-        h2 = torch.stack([torch.diag(pv), torch.diag(zc * pv)])
+        pu = torch.exp(torch.complex(torch.zeros_like(hu).unsqueeze(1) * z, -tau * hu.unsqueeze(1) * z))
+        pv = torch.exp(torch.complex(torch.zeros_like(hv).unsqueeze(1) * z, -tau * hv.unsqueeze(1) * z))
+        c = torch.cos(tau * J).to(torch.complex128).unsqueeze(1)
+        sn = torch.sin(tau * J).to(torch.complex128).unsqueeze(1)
+        h1 = torch.stack([torch.diag_embed(c * pu), torch.diag_embed(-1j * sn * zc * pu)], dim=1)
+        h2 = torch.stack([torch.diag_embed(pv), torch.diag_embed(zc * pv)], dim=1)
         return h1, h2
 
     # ------------------------------------------------------- operations
-    def apply1_all(self, gam, G):
-        out = []
-        for T in gam:
-            t = torch.tensordot(T, G, dims=([T.dim() - 1], [1]))
-            out.append(t / torch.linalg.vector_norm(t))
+    @staticmethod
+    def _groups(keys) -> Dict:
+        out: Dict = {}
+        for i, k in enumerate(keys):
+            out.setdefault(k, []).append(i)
         return out
 
-    def _prepare(self, T, lams: Sequence[torch.Tensor], half, index: int):
-        """tensor_ops.py:265-283 up to the QR: lambda-scale the other bonds, apply
-        the half gate (phys contracted with its input, rank merged into bond
-        ``index`` bond-major, normalised), bond ``index`` moved last."""
-        k = T.dim() - 1
-        for f, l in enumerate(lams):
-            if f != index:
-                T = T * _bcast(l.to(T.dtype), f, k + 1)
-        shape = list(T.shape)
-        shape[index] *= half.shape[0]
-        T = torch.tensordot(T, half, dims=([k], [2]))  # (..bonds.., r, o)
-        n = T.dim()
-        T = T.permute(*range(index + 1), n - 2, *range(index + 1, n - 2), n - 1).reshape(shape)
-        T = T / torch.linalg.vector_norm(T)
-        return torch.movedim(T, index, -1)
+    def apply1_all(self, gam, G):
+        """tensor_graph.py:268-275 on every node, batched by tensor shape."""
+        out = list(gam)
+        for shape, vs in self._groups([tuple(g.shape) for g in gam]).items():
+            X = torch.stack([gam[v] for v in vs])
+            X = torch.tensordot(X, G, dims=([X.dim() - 1], [1]))
+            X = X / torch.linalg.vector_norm(X.reshape(len(vs), -1), dim=1).reshape((-1,) + (1,) * (X.dim() - 1))
+            for i, v in enumerate(vs):
+                out[v] = X[i]
+        return out
 
-    def simple_update(self, gam, lam, gate, h1, h2):
-        """tensor_ops.py:318-389 for one gate (rank = min(max_chi, available))."""
-        e, a, ia, b, ib = gate[:5]
-        la = [lam[f] for f in self.node_edges[a]]
-        lb = [lam[f] for f in self.node_edges[b]]
-        Pa = self._prepare(gam[a], la, h1, ia)
-        Pb = self._prepare(gam[b], lb, h2, ib)
+    def _prepare(self, X, others: List[torch.Tensor], half):
+        """tensor_ops.py:265-283 up to the QR for a batch: X (B, c_e, others.., d)
+        with the gate bond first; lambda-scale the other bonds, apply the half
+        gate (phys contracted with its input, rank merged into the gate bond
+        bond-major, normalised), gate bond moved last -> (B, rows, c_e r)."""
+        B = X.shape[0]
+        nd = X.dim()
+        for p, L in enumerate(others):
+            shape = [B] + [1] * (nd - 1)
+            shape[p + 2] = L.shape[1]
+            X = X * L.reshape(shape).to(X.dtype)
+        r = half.shape[1]
+        ax = "xyzwuvtq"[: nd - 2]
+        X = torch.einsum("b" + ax + "i,broi->b" + ax + "ro", X, half)
+        # (B, c_e, others.., r, o) -> (B, c_e, r, others.., o) -> merge (c_e r)
+        X = torch.movedim(X, nd - 1, 2)
+        ce = X.shape[1]
+        X = X.reshape((B, ce * r) + tuple(X.shape[3:]))
+        X = X / torch.linalg.vector_norm(X.reshape(B, -1), dim=1).reshape((B,) + (1,) * (X.dim() - 1))
+        X = torch.movedim(X, 1, -1)
+        return X
+
+    def _simple_update_group(self, gam, lam, idx: List[int], h1, h2):
+        """tensor_ops.py:318-389 for node-disjoint gates of identical shapes,
+        as one batch (rank = min(max_chi, available))."""
+        gts = [self.gates[j] for j in idx]
+        B = len(gts)
+
+        def side(node_pos, bond_pos, half):
+            X = torch.stack([torch.movedim(gam[g[node_pos]], g[bond_pos], 0) for g in gts])
+            nb = X.dim() - 2  # bonds of the node
+            others = []
+            for p in range(nb - 1):
+                others.append(torch.stack([lam[[f for q, f in enumerate(self.node_edges[g[node_pos]])
+                                                if q != g[bond_pos]][p]] for g in gts]))
+            P = self._prepare(X, others, half)
+            return P, others
+
+        Pa, oa = side(1, 2, h1)
+        Pb, ob = side(3, 4, h2)
         K = Pa.shape[-1]
-        d = lam[e].repeat_interleave(h1.shape[0]).to(torch.complex128)
-        Wa, S, Wb = product_svd(Pa.reshape(-1, K) * d.unsqueeze(0), Pb.reshape(-1, K))
+        d = torch.stack([lam[g[0]] for g in gts]).repeat_interleave(h1.shape[1], dim=1).to(torch.complex128)
+        Wa, S, Wb = product_svd(Pa.reshape(B, -1, K) * d.unsqueeze(1), Pb.reshape(B, -1, K))
         lmbd = (S > self.eps).to(S.dtype) * S
-        rank = min(self.max_chi, S.shape[0])
+        rank = min(self.max_chi, S.shape[-1])
 
-        def finish(W, P, lams, index):
-            q = W[:, :rank].reshape(P.shape[:-1] + (rank,))
+        def finish(W, P, others):
+            q = W[..., :rank].reshape(P.shape[:-1] + (rank,))  # (B, others.., d, rank)
             nd = q.dim()
-            others = [l for f, l in enumerate(lams) if f != index]
-            for f, l in enumerate(others):
-                q = q * _bcast(safe_inverse(l, self.eps).to(q.dtype), f, nd)
-            return torch.movedim(q, nd - 1, index)  # (others.., phys, rank) -> rank at ``index``
+            for p, L in enumerate(others):
+                shape = [B] + [1] * (nd - 1)
+                shape[p + 1] = L.shape[1]
+                q = q * safe_inverse(L, self.eps).reshape(shape).to(q.dtype)
+            return q
 
+        qa = finish(Wa, Pa, oa)
+        qb = finish(Wb, Pb, ob)
         gam = list(gam)
         lam = list(lam)
-        gam[a] = finish(Wa, Pa, la, ia)
-        gam[b] = finish(Wb, Pb, lb, ib)
-        lam[e] = lmbd[:rank]
+        for i, g in enumerate(gts):
+            gam[g[1]] = torch.movedim(qa[i], qa.dim() - 2, g[2])
+            gam[g[3]] = torch.movedim(qb[i], qb.dim() - 2, g[4])
+            lam[g[0]] = lmbd[i, :rank]
         return gam, lam
 
     def coupling_layer(self, gam, lam, tau):
-        for gate in self.gates:
-            h1, h2 = self.coupling_halves(tau, *gate[5:])
-            gam, lam = self.simple_update(gam, lam, gate, h1, h2)
+        """All coupling gates in pair order, a level of node-disjoint gates
+        at a time, each level batched by shape."""
+        for level in self.levels:
+            keys = []
+            for j in level:
+                e, a, ia, b, ib = self.gates[j][:5]
+                keys.append((tuple(torch.movedim(gam[a], ia, 0).shape), tuple(torch.movedim(gam[b], ib, 0).shape)))
+            for _, pos in self._groups(keys).items():
+                idx = [level[p] for p in pos]
+                h1, h2 = self.coupling_halves(tau, idx)
+                gam, lam = self._simple_update_group(gam, lam, idx, h1, h2)
         return gam, lam
 
     def _problem(self, lam) -> FixedPointProblem:
@@ -199,15 +253,24 @@ class AnnealingGradient:
         return FixedPointProblem(self.graph, topo=self.topo)
 
     def regauge(self, gam, lam):
-        """Symmetric gauge, BP fixed point, Vidal gauge."""
+        """Symmetric gauge, BP fixed point, Vidal gauge (nodes batched by tensor
+        shape, edges by bond dimension)."""
         P = self._problem(lam)
         L = P.layout
-        Ts = []
-        for v, G in enumerate(gam):
-            T = G
-            for f, ei in enumerate(self.node_edges[v]):
-                T = T * _bcast(safe_sqrt_truncate(lam[ei], self.eps).to(T.dtype), f, G.dim())
-            Ts.append(T / torch.linalg.vector_norm(T))
+        N = len(gam)
+        node_groups = self._groups([tuple(g.shape) for g in gam])
+        Ts: List = [None] * N
+        for shape, vs in node_groups.items():
+            X = torch.stack([gam[v] for v in vs])
+            nd = X.dim()
+            for f in range(nd - 2):
+                Lf = torch.stack([safe_sqrt_truncate(lam[self.node_edges[v][f]], self.eps) for v in vs])
+                sh = [len(vs)] + [1] * (nd - 1)
+                sh[f + 1] = Lf.shape[1]
+                X = X * Lf.reshape(sh).to(X.dtype)
+            X = X / torch.linalg.vector_norm(X.reshape(len(vs), -1), dim=1).reshape((-1,) + (1,) * (nd - 1))
+            for i, v in enumerate(vs):
+                Ts[v] = X[i]
         T_arena = torch.cat([T.reshape(-1) for T in Ts])
         with torch.no_grad():
             n2e0 = torch.zeros(max(L.msg_elems, 1), dtype=torch.complex128, device=self.device)
@@ -220,41 +283,50 @@ class AnnealingGradient:
         self.last_bp_sweeps.append(P.last_sweeps)
         msgs = P.messages(n2e)
         orth: Dict[Tuple[int, int], torch.Tensor] = {}
-        new_lam = []
-        for a, ia, b, ib in self.edge_ends:
-            Gf, Gb, l = self._edge_svd(msgs[int(L.node_half[a]) + ia], msgs[int(L.node_half[b]) + ib])
-            orth[(a, ia)] = Gf
-            orth[(b, ib)] = Gb
-            new_lam.append(l)
-        new_gam = []
-        for v, T in enumerate(Ts):
-            t = T
-            for f in range(T.dim() - 1):
-                t = torch.tensordot(t, orth[(v, f)], dims=([0], [0]))
-            t = t.permute(*range(1, t.dim()), 0)
-            new_gam.append(t / torch.linalg.vector_norm(t))
+        new_lam: List = [None] * len(self.edges)
+        for c, es in self._groups([int(l.shape[0]) for l in lam]).items():
+            ends = [self.edge_ends[e] for e in es]
+            mf = torch.stack([msgs[int(L.node_half[a]) + ia] for a, ia, _, _ in ends])
+            mb = torch.stack([msgs[int(L.node_half[b]) + ib] for _, _, b, ib in ends])
+            Gf, Gb, lb = self._edge_svd(mf, mb)
+            for i, (e, (a, ia, b, ib)) in enumerate(zip(es, ends)):
+                orth[(a, ia)] = Gf[i]
+                orth[(b, ib)] = Gb[i]
+                new_lam[e] = lb[i]
+        new_gam: List = [None] * N
+        for shape, vs in node_groups.items():
+            X = torch.stack([Ts[v] for v in vs])
+            nb = X.dim() - 2
+            ax = "abcdefgh"[:nb]
+            out = "pqrstuvw"[:nb]
+            ops = [X] + [torch.stack([orth[(v, f)] for v in vs]) for f in range(nb)]
+            spec = "n" + ax + "s," + ",".join("n" + ax[f] + out[f] for f in range(nb)) + "->n" + out + "s"
+            X = torch.einsum(spec, *ops)
+            X = X / torch.linalg.vector_norm(X.reshape(len(vs), -1), dim=1).reshape((-1,) + (1,) * (nb + 1))
+            for i, v in enumerate(vs):
+                new_gam[v] = X[i]
         return new_gam, new_lam
 
     def _edge_svd(self, mf, mb):
-        """tensor_ops.py:108-130."""
+        """tensor_ops.py:108-130 for a batch of edges (messages (B, c, c))."""
         eps = self.eps
         lf, uf = eigh(0.5 * (mf + mf.mH))
         lb, ub = eigh(0.5 * (mb + mb.mH))
 
         def sq(l, u, inv):
             w = torch.sqrt(safe_inverse(l, eps)) if inv else safe_sqrt_truncate(l, eps)
-            return (u * w.to(u.dtype).unsqueeze(0)) @ u.mH
+            return (u * w.to(u.dtype).unsqueeze(-2)) @ u.mH
 
         m_sq_inv_f, m_sq_inv_b = sq(lf, uf, True), sq(lb, ub, True)
-        u, s, vh = svd(sq(lf, uf, False) @ sq(lb, ub, False).T)
-        s = s / torch.linalg.vector_norm(s)
+        u, s, vh = svd(sq(lf, uf, False) @ sq(lb, ub, False).mT)
+        s = s / torch.linalg.vector_norm(s, dim=-1, keepdim=True)
         keep = (s > eps).to(s.dtype)
         s = keep * s
-        u = u * keep.to(u.dtype).unsqueeze(0)
-        u = u / torch.linalg.vector_norm(u)
-        vh = vh * keep.to(vh.dtype).unsqueeze(1)
-        vh = vh / torch.linalg.vector_norm(vh)
-        return m_sq_inv_f @ u, m_sq_inv_b @ vh.T, s
+        u = u * keep.to(u.dtype).unsqueeze(-2)
+        u = u / torch.linalg.vector_norm(u, dim=(-2, -1), keepdim=True)
+        vh = vh * keep.to(vh.dtype).unsqueeze(-1)
+        vh = vh / torch.linalg.vector_norm(vh, dim=(-2, -1), keepdim=True)
+        return m_sq_inv_f @ u, m_sq_inv_b @ vh.mT, s
 
     def step(self, gam, lam, s_t, first: bool):
         tau_m = -self.dt * (1.0 - s_t)

@@ -80,7 +80,7 @@ class SVD(torch.autograd.Function):
 
 
 class ProductSVD(torch.autograd.Function):
-    """SVD of Theta = X Y^T from its factors X (m x K), Y (n x K):
+    """SVD of Theta = X Y^T from its factors X (..., m, K), Y (..., n, K):
     Theta = U diag(S) W^T with U (m x k), W (n x k), k = min(m, n, K).
 
     Forward: X = Qx Rx, Y = Qy Ry (reduced QR), SVD of the core Rx Ry^T
@@ -96,9 +96,9 @@ class ProductSVD(torch.autograd.Function):
     def forward(ctx, X, Y, broadening: float = DEFAULT_BROADENING):
         Qx, Rx = torch.linalg.qr(X, mode="reduced")
         Qy, Ry = torch.linalg.qr(Y, mode="reduced")
-        Uc, S, Vch = torch.linalg.svd(Rx @ Ry.T, full_matrices=False)
+        Uc, S, Vch = torch.linalg.svd(Rx @ Ry.mT, full_matrices=False)
         U = Qx @ Uc
-        W = Qy @ Vch.T
+        W = Qy @ Vch.mT
         ctx.save_for_backward(X, Y, U, S, W)
         ctx.broadening = broadening
         return U, S, W
@@ -107,10 +107,10 @@ class ProductSVD(torch.autograd.Function):
     def backward(ctx, gU, gS, gW):
         X, Y, U, S, W = ctx.saved_tensors
         m, n = X.shape[-2], Y.shape[-2]
-        Vh = W.T  # Theta = U S W^T = U S Vh
-        gVh = None if gW is None else gW.T
+        Vh = W.mT  # Theta = U S W^T = U S Vh
+        gVh = None if gW is None else gW.mT
         gT = svd_adjoint(U, S, Vh, gU, gS, gVh, ctx.broadening, m, n)
-        return gT @ Y.conj(), gT.T @ X.conj(), None
+        return gT @ Y.conj(), gT.mT @ X.conj(), None
 
 
 class EighH(torch.autograd.Function):

@@ -90,3 +90,19 @@ def test_degenerate_spectra_stay_finite():
     w, V = eigh(I)
     (gI,) = torch.autograd.grad(w.sum() + (V.abs() ** 2).sum(), I)
     assert torch.isfinite(gI).all()
+
+
+def test_product_svd_batched_equals_unbatched():
+    g = torch.Generator().manual_seed(7)
+    X = torch.randn(4, 9, 6, dtype=torch.complex128, generator=g, requires_grad=True)
+    Y = torch.randn(4, 8, 6, dtype=torch.complex128, generator=g, requires_grad=True)
+    M = torch.randn(4, 9, 8, dtype=torch.complex128, generator=g)
+
+    def loss(U, S, W, M):
+        return torch.einsum("...ij,...ik,...jk->...k", M, U.conj(), W.conj()).real.sum() + S.sum()
+
+    gb = torch.autograd.grad(loss(*product_svd(X, Y), M), (X, Y))
+    for b in range(4):
+        gs = torch.autograd.grad(loss(*product_svd(X[b], Y[b]), M[b]), (X, Y))
+        for a, c in zip(gb, gs):
+            assert float((a[b] - c[b]).abs().max()) < 1e-12
