@@ -259,12 +259,24 @@ class AnnealingGradient:
         L = P.layout
         N = len(gam)
         node_groups = self._groups([tuple(g.shape) for g in gam])
+        # sqrt(truncated lambda) of every edge, once (one stacked op when all
+        # bonds have the same dimension)
+        if len({int(l.shape[0]) for l in lam}) == 1:
+            sl_stack = safe_sqrt_truncate(torch.stack(lam), self.eps)
+            sqrt_lam = None
+        else:
+            sl_stack = None
+            sqrt_lam = [safe_sqrt_truncate(l, self.eps) for l in lam]
         Ts: List = [None] * N
         for shape, vs in node_groups.items():
             X = torch.stack([gam[v] for v in vs])
             nd = X.dim()
             for f in range(nd - 2):
-                Lf = torch.stack([safe_sqrt_truncate(lam[self.node_edges[v][f]], self.eps) for v in vs])
+                if sl_stack is not None:
+                    ix = torch.as_tensor([self.node_edges[v][f] for v in vs], device=self.device)
+                    Lf = sl_stack[ix]
+                else:
+                    Lf = torch.stack([sqrt_lam[self.node_edges[v][f]] for v in vs])
                 sh = [len(vs)] + [1] * (nd - 1)
                 sh[f + 1] = Lf.shape[1]
                 X = X * Lf.reshape(sh).to(X.dtype)
@@ -274,8 +286,15 @@ class AnnealingGradient:
         T_arena = torch.cat([T.reshape(-1) for T in Ts])
         with torch.no_grad():
             n2e0 = torch.zeros(max(L.msg_elems, 1), dtype=torch.complex128, device=self.device)
-            for h in range(L.n_halves):
-                L.message_view(n2e0, h).copy_(torch.diag(lam[int(L.half_edge[h])].to(torch.complex128)))
+            chis = {int(l.shape[0]) for l in lam}
+            if len(chis) == 1 and L.exact() and L.n_halves:
+                c = chis.pop()
+                lam_e = torch.stack([l.detach() for l in lam]).to(torch.complex128)
+                he = torch.as_tensor(L.half_edge.astype(np.int64), device=self.device)
+                n2e0[: L.n_halves * c * c] = torch.diag_embed(lam_e[he]).reshape(-1)
+            else:
+                for h in range(L.n_halves):
+                    L.message_view(n2e0, h).copy_(torch.diag(lam[int(L.half_edge[h])].to(torch.complex128)))
         if T_arena.requires_grad:
             n2e, _ = BPFixedPoint.apply(T_arena, P, n2e0, self.bp_tol, self.bp_max, self.bp_tol, self.bp_max)
         else:

@@ -18,6 +18,30 @@ import torch
 DEFAULT_BROADENING = 1e-24
 
 
+def qr(X: torch.Tensor):
+    """Reduced QR of a batch of matrices (..., m, k): the library's batched
+    Householder kernel for complex128 tensors on the GPU (torch.linalg.qr
+    elsewhere, e.g. CPU tests). Not differentiated."""
+    if not (X.is_cuda and X.dtype == torch.complex128):
+        return torch.linalg.qr(X, mode="reduced")
+    from . import _lib
+
+    m, k = X.shape[-2], X.shape[-1]
+    kk = min(m, k)
+    lead = X.shape[:-2]
+    batch = 1
+    for d in lead:
+        batch *= int(d)
+    A = X.detach().reshape(batch, m, k).contiguous()
+    Q = torch.empty((batch, m, kk), dtype=X.dtype, device=X.device)
+    R = torch.empty((batch, kk, k), dtype=X.dtype, device=X.device)
+    nb = _lib.lib().dqz_qr_batched_scratch_bytes(batch, m, k)
+    scratch = torch.empty(max(int(nb), 1), dtype=torch.uint8, device=X.device)
+    _lib.call("dqz_qr_batched", A.data_ptr(), batch, m, k, Q.data_ptr(), R.data_ptr(), scratch.data_ptr(),
+              _lib.stream_handle())
+    return Q.reshape(lead + (m, kk)), R.reshape(lead + (kk, k))
+
+
 def _inv_lorentz(x: torch.Tensor, b: float) -> torch.Tensor:
     return x / (x * x + b)
 
@@ -94,8 +118,8 @@ class ProductSVD(torch.autograd.Function):
 
     @staticmethod
     def forward(ctx, X, Y, broadening: float = DEFAULT_BROADENING):
-        Qx, Rx = torch.linalg.qr(X, mode="reduced")
-        Qy, Ry = torch.linalg.qr(Y, mode="reduced")
+        Qx, Rx = qr(X)
+        Qy, Ry = qr(Y)
         Uc, S, Vch = torch.linalg.svd(Rx @ Ry.mT, full_matrices=False)
         U = Qx @ Uc
         W = Qy @ Vch.mT

@@ -155,6 +155,15 @@ int dqz_bp_node_vjp(const dqz_graph_t *g, const void *tensors, const void *e2n, 
                     int32_t max_chi, void *scratch, cudaStream_t stream);
 size_t dqz_bp_node_vjp_scratch_bytes(int32_t n_nodes, int32_t max_size);
 
+/* ---- Batched reduced QR (the QR of tensor_ops.py:288, LAPACK conventions) --
+ * For each of `batch` row-major m x k complex128 matrices A_b: A_b = Q_b R_b with
+ * Q_b (m x min(m,k), orthonormal columns, row-major) and R_b (min(m,k) x k,
+ * upper trapezoidal, row-major). Householder reflectors as zgeqr2, Q formed
+ * as zung2r. Used by the differentiable two-site decomposition. */
+int dqz_qr_batched(const void *a, int64_t batch, int32_t m, int32_t k, void *q, void *r, void *scratch,
+                   cudaStream_t stream);
+size_t dqz_qr_batched_scratch_bytes(int64_t batch, int32_t m, int32_t k);
+
 /* ---- Vidal gauge (mappings/vidal_gauge.py:21-63, tensor_ops.py:88-130) ---- */
 
 /* Per edge: eigendecompose both node->edge messages, build sqrt / safe inverse

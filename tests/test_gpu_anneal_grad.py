@@ -108,3 +108,23 @@ def test_gradient_matches_finite_differences(k):
         fd = (ag.energy_value(s + h * d) - ag.energy_value(s - h * d)) / (2 * h)
         ad = float(grad @ d)
         assert abs(ad - fd) <= 1e-5 * max(abs(fd), 1e-3), (ad, fd)
+
+
+@pytest.mark.parametrize("batch,m,k", [(3, 512, 32), (600, 40, 8), (5, 6, 9), (2, 7, 7)])
+def test_batched_qr_kernel(batch, m, k):
+    """dqz_qr_batched: Q R = A, Q^H Q = I, R upper trapezoidal, |diag R| equal to
+    LAPACK's (torch.linalg.qr), 1e-12 relative; more matrices than CTAs."""
+    from dequantizer_b200.linalg_ad import qr
+
+    gen = torch.Generator(device="cuda").manual_seed(batch + m + k)
+    A = torch.randn(batch, m, k, dtype=torch.complex128, device="cuda", generator=gen)
+    Q, R = qr(A)
+    kk = min(m, k)
+    assert Q.shape == (batch, m, kk) and R.shape == (batch, kk, k)
+    assert float((Q @ R - A).abs().max() / A.abs().max()) < 1e-12
+    eye = torch.eye(kk, dtype=A.dtype, device=A.device)
+    assert float((Q.mH @ Q - eye).abs().max()) < 1e-12
+    assert float(torch.tril(R, diagonal=-1).abs().max()) == 0.0
+    Rt = torch.linalg.qr(A, mode="reduced")[1]
+    d1, d2 = torch.diagonal(R, dim1=-2, dim2=-1).abs(), torch.diagonal(Rt, dim1=-2, dim2=-1).abs()
+    assert float((d1 - d2).abs().max() / d2.abs().max()) < 1e-12
