@@ -29,6 +29,12 @@ Differences from the reference loop that keep the map smooth in s:
   * the truncated two-site decomposition is the SVD of
     Theta = A_u diag(lambda_e x 1_r) A_v^T through ``product_svd`` (the
     reference's QR + core SVD forward, with the adjoint of Theta's own SVD).
+Non-differentiable point: a coupling step with s_t = 0 exactly applies the
+identity, and the Schmidt values it would create grow like |tau|; the
+canonical form (square roots and safe inverses of lambda) is not
+differentiable there although E is, and the reverse pass returns the
+derivative with that bond component held at zero (dE/ds_t = 0 from the
+coupling). Schedules should keep s_t > 0 (e.g. midpoint values (t + 1/2)/N).
 Reverse pass: the forward stores (Gamma, lambda) every ``checkpoint_every``
 steps; segments are recomputed under autograd in reverse order and
 differentiated with the hand-written SVD / eigh adjoints of ``linalg_ad`` and

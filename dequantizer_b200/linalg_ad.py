@@ -15,7 +15,10 @@ on the choice of basis inside the block (gauge-invariant ones).
 
 import torch
 
-DEFAULT_BROADENING = 1e-24
+# The spectra differentiated here are O(1) (normalised two-site matrices,
+# trace-1 messages): 1e-28 keeps gaps above ~1e-13 exact and damps
+# rounding-level gaps (~1e-16), whose rotation terms are noise.
+DEFAULT_BROADENING = 1e-28
 
 
 def qr(X: torch.Tensor):

@@ -128,3 +128,25 @@ def test_batched_qr_kernel(batch, m, k):
     Rt = torch.linalg.qr(A, mode="reduced")[1]
     d1, d2 = torch.diagonal(R, dim1=-2, dim2=-1).abs(), torch.diagonal(Rt, dim1=-2, dim2=-1).abs()
     assert float((d1 - d2).abs().max() / d2.abs().max()) < 1e-12
+
+
+def test_zero_coupling_step_is_the_documented_nondifferentiable_point():
+    """s_0 = 0 makes the first coupling layer the identity: the reverse pass
+    returns 0 for that component (the Schmidt values there grow like |tau|),
+    while every other component still matches finite differences; just inside
+    the interval (s_0 = 0.01) all components match."""
+    energy = W.random_regular_energy(8, 3, seed=21, field_std=0.0)
+    h = 1e-4
+    for s0 in (0.0, 0.01):
+        s = np.linspace(0.0, 1.0, 6)
+        s[0] = s0
+        ag = AnnealingGradient(energy, max_chi=4, dt=DT, checkpoint_every=2, bp_tol=1e-14)
+        _, g = ag.value_and_grad(s)
+        for j in range(3):
+            d = np.zeros(6)
+            d[j] = 1.0
+            fd = (ag.energy_value(s + h * d) - ag.energy_value(s - h * d)) / (2 * h)
+            if s0 == 0.0 and j == 0:
+                assert abs(g[0]) < 1e-12 and abs(fd) > 1e-2
+            else:
+                assert abs(g[j] - fd) <= 1e-5 * max(abs(fd), 1e-3), (s0, j, g[j], fd)
