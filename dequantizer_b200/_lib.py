@@ -88,6 +88,8 @@ _SIGNATURES = {
     "dqz_segment_distance": (ctypes.c_int, [_P, _P, _P, _I, _P, _P, _P]),
     "dqz_bp_node_vjp": (ctypes.c_int, [_G, _P, _P, _P, _P, _P, _P, _I, _I, _I, _P, _P]),
     "dqz_qr_batched": (ctypes.c_int, [_P, ctypes.c_int64, _I, _I, _P, _P, _P, _P]),
+    "dqz_set_tuning": (ctypes.c_int, [_I, _I]),
+    "dqz_get_tuning": (ctypes.c_int32, [_I]),
     "dqz_qr_batched_scratch_bytes": (_S, [ctypes.c_int64, _I, _I]),
     "dqz_bp_node_vjp_scratch_bytes": (_S, [_I, _I]),
     "dqz_vidal_edges": (ctypes.c_int, [_G, _P, _D, _P, _P, _I, _P, _I, _P, _P]),

@@ -50,7 +50,11 @@ class BatchedAnnealer:
         max_belief_propagation_iterations: Optional[int] = 100,
         schedule: str = "sync",
         key: int = 0,
+        autotune: bool = False,
     ):
+        """``autotune``: time the gauge kernels' launch shapes on the first
+        regauge of every new maximal bond dimension (``autotune.tune_gauge``,
+        cached on disk) and use the fastest."""
         if schedule not in ("sync", "flooding"):
             raise ValueError("batched annealing runs the synchronous or flooding BP schedule")
         if not torch.cuda.is_available():
@@ -61,6 +65,8 @@ class BatchedAnnealer:
         self.accuracy = float(accuracy)
         self.max_iters = max_belief_propagation_iterations
         self._rng = np.random.default_rng(key)
+        self.autotune = bool(autotune)
+        self._tuned_chi = set()
         # ---- union graph, traversal = concatenated per-instance DFS traversals
         self.graph = TensorGraph()
         trav: List = []
@@ -281,6 +287,11 @@ class BatchedAnnealer:
         n2e, e2n = L.new_msg_arena(), L.new_msg_arena()
         _lib.call("dqz_lambdas_to_messages", L.gptr, self.lam.data_ptr(), n2e.data_ptr(), e2n.data_ptr(),
                   L.max_chi(), _lib.stream_handle())
+        if self.autotune and L.max_chi() not in self._tuned_chi:
+            from .autotune import tune_gauge
+
+            tune_gauge(L, T, n2e, EPS)
+            self._tuned_chi.add(L.max_chi())
         G = torch.empty_like(T)
         lam = L.new_lam_arena()
         orth = torch.empty(max(L.msg_elems, 1), dtype=torch.complex128, device=L.device)

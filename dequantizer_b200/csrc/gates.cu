@@ -371,6 +371,8 @@ extern "C" int dqz_simple_update(const dqz_graph_t *g, void *tensors, double *la
   if (smem > SMEM_LIMIT) return DQZ_ERR_UNSUPPORTED;
   DQZ_SMEM_ATTR_ONCE(simple_update_kernel, SMEM_LIMIT);
   int grid = n < SU_GRID_MAX ? n : SU_GRID_MAX;
+  const int tuned = dqz_get_tuning(DQZ_TUNE_SU_GRID);  // never above the scratch sizing (SU_GRID_MAX)
+  if (tuned > 0 && tuned < grid) grid = tuned;
   simple_update_kernel<<<grid, GATE_THREADS, smem, stream>>>(*g, (cd *)tensors, lambdas, edges, ctrl_is_first,
                                                              (const cd *)halves, ranks, n, eps, max_rank, max_rows,
                                                              max_cols, err, entropy, (cd *)scratch);

@@ -579,10 +579,12 @@ extern "C" int dqz_vidal_edges(const dqz_graph_t *g, const void *n2e, double eps
   if (edges && (n_sel < 0 || n_sel > g->n_edges)) return DQZ_ERR_ARG;
   const int total = edges ? n_sel : g->n_edges;
   if (total == 0) return DQZ_OK;
-  if (max_chi <= WARP_MAX_CHI) {
+  if (max_chi <= WARP_MAX_CHI && dqz_get_tuning(DQZ_TUNE_GAUGE_PATH) != 2) {
     const size_t per = warp_edge_bytes(max_chi);
     int wpb = (int)(WARP_BLOCK_SMEM / per);
     wpb = wpb < 1 ? 1 : (wpb > GAUGE_THREADS / 32 ? GAUGE_THREADS / 32 : wpb);
+    const int tuned = dqz_get_tuning(DQZ_TUNE_GAUGE_EDGE_WARPS);
+    if (tuned > 0 && (size_t)tuned * per <= SMEM_LIMIT) wpb = tuned;
     DQZ_SMEM_ATTR_ONCE(vidal_edges_warp_kernel, SMEM_LIMIT);
     vidal_edges_warp_kernel<<<(total + wpb - 1) / wpb, 32 * wpb, wpb * per, stream>>>(
         *g, (const cd *)n2e, eps, (cd *)orth, lambdas, max_chi, edges, total);
@@ -638,10 +640,13 @@ extern "C" int dqz_vidal_distance(const dqz_graph_t *g, const void *tensors, con
   if (halves && (n_sel < 0 || n_sel > nh)) return DQZ_ERR_ARG;
   const int total = halves ? n_sel : nh;
   if (total > 0) {
-    if (max_chi <= WARP_MAX_CHI && max_slice > 0 && max_slice <= WARP_MAX_SLICE) {
+    if (max_chi <= WARP_MAX_CHI && max_slice > 0 && max_slice <= WARP_MAX_SLICE &&
+        dqz_get_tuning(DQZ_TUNE_GAUGE_PATH) != 2) {
       const size_t per = warp_vd_bytes(max_chi, max_slice);
       int wpb = (int)(WARP_BLOCK_SMEM / per);
       wpb = wpb < 1 ? 1 : (wpb > GAUGE_THREADS / 32 ? GAUGE_THREADS / 32 : wpb);
+      const int tuned = dqz_get_tuning(DQZ_TUNE_GAUGE_DIST_WARPS);
+      if (tuned > 0 && (size_t)tuned * per <= SMEM_LIMIT) wpb = tuned;
       DQZ_SMEM_ATTR_ONCE(vidal_distance_warp_kernel, SMEM_LIMIT);
       vidal_distance_warp_kernel<<<(total + wpb - 1) / wpb, 32 * wpb, wpb * per, stream>>>(
           *g, (const cd *)tensors, lambdas, eps, partial, max_chi, max_slice, halves, total);

@@ -69,6 +69,19 @@ typedef struct {
 int dqz_version(void);
 int dqz_device_supported(int device); /* 1 when the device is sm_100 */
 
+/* ---- Launch-shape knobs (no reference counterpart) -------------------------
+ * Read by the host side of the entry points at every launch; 0 means the
+ * built-in rule. Set by the autotuner (dequantizer_b200/autotune.py), which
+ * times the candidates on the caller's shapes. Process-wide, not thread-safe
+ * against concurrent launches from other host threads. */
+#define DQZ_TUNE_GAUGE_EDGE_WARPS 0 /* warps per CTA of the one-warp vidal_edges kernel (1..8)   */
+#define DQZ_TUNE_GAUGE_DIST_WARPS 1 /* warps per CTA of the one-warp vidal_distance kernel (1..8) */
+#define DQZ_TUNE_GAUGE_PATH 2       /* 1: one-warp gauge kernels where they apply, 2: one CTA per item */
+#define DQZ_TUNE_SU_GRID 3          /* CTAs of simple_update (>= 1), jobs loop over the grid     */
+#define DQZ_TUNE_COUNT 4
+int dqz_set_tuning(int32_t knob, int32_t value); /* DQZ_ERR_ARG for an unknown knob or value < 0 */
+int32_t dqz_get_tuning(int32_t knob);            /* -1 for an unknown knob */
+
 /* ---- Belief propagation (dequantizer/src/mappings/belief_propagation.py:24-64,
  *      dequantizer/src/tensor_ops.py:36-76) ---------------------------------- */
 
