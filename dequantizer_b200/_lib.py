@@ -89,6 +89,12 @@ _SIGNATURES = {
     "dqz_bp_node_vjp": (ctypes.c_int, [_G, _P, _P, _P, _P, _P, _P, _I, _I, _I, _P, _P]),
     "dqz_qr_batched": (ctypes.c_int, [_P, ctypes.c_int64, _I, _I, _P, _P, _P, _P]),
     "dqz_set_tuning": (ctypes.c_int, [_I, _I]),
+    "dqz_sv_set_basis": (ctypes.c_int, [_P, _I, ctypes.c_int64, _P]),
+    "dqz_sv_apply1": (ctypes.c_int, [_P, _I, _I, _P, _P]),
+    "dqz_sv_apply2": (ctypes.c_int, [_P, _I, _I, _I, _P, _P]),
+    "dqz_sv_density1": (ctypes.c_int, [_P, _I, _I, _P, _P, _P]),
+    "dqz_sv_density_scratch_bytes": (_S, [_I]),
+    "dqz_sv_project": (ctypes.c_int, [_P, _I, _I, _I, _D, _P]),
     "dqz_get_tuning": (ctypes.c_int32, [_I]),
     "dqz_qr_batched_scratch_bytes": (_S, [ctypes.c_int64, _I, _I]),
     "dqz_bp_node_vjp_scratch_bytes": (_S, [_I, _I]),

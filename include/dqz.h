@@ -177,6 +177,21 @@ int dqz_qr_batched(const void *a, int64_t batch, int32_t m, int32_t k, void *q, 
                    cudaStream_t stream);
 size_t dqz_qr_batched_scratch_bytes(int64_t batch, int32_t m, int32_t k);
 
+/* ---- Dense state vector (quantum_emulator/exact_quantum_emulator.py:11-147) --
+ * complex128 state of 2^n amplitudes in device memory; the qubit at position p
+ * (traversal order of the nodes) is bit n-1-p of the amplitude index.
+ * Gates are HOST arrays of complex128 (re, im interleaved): 2x2 g[o][i] for
+ * apply1, 2x2x2x2 g[o1][o2][i1][i2] for apply2 (first qubit = pos1). */
+#define DQZ_SV_MAX_QUBITS 34
+int dqz_sv_set_basis(void *state, int32_t n, int64_t index, cudaStream_t stream);
+int dqz_sv_apply1(void *state, int32_t n, int32_t pos, const double *gate, cudaStream_t stream);
+int dqz_sv_apply2(void *state, int32_t n, int32_t pos1, int32_t pos2, const double *gate, cudaStream_t stream);
+/* rho (device, 2x2 complex128) = one-qubit reduced density matrix of position pos. */
+int dqz_sv_density1(const void *state, int32_t n, int32_t pos, void *rho, void *scratch, cudaStream_t stream);
+size_t dqz_sv_density_scratch_bytes(int32_t n);
+/* Projects position pos onto |result> and multiplies the state by scale. */
+int dqz_sv_project(void *state, int32_t n, int32_t pos, int32_t result, double scale, cudaStream_t stream);
+
 /* ---- Vidal gauge (mappings/vidal_gauge.py:21-63, tensor_ops.py:88-130) ---- */
 
 /* Per edge: eigendecompose both node->edge messages, build sqrt / safe inverse
