@@ -386,6 +386,62 @@ class BatchedAnnealer:
             out.append(rho[idx])
         return out
 
+    def sample_measurements(self, samples: Optional[np.ndarray] = None, seed: int = 0) -> List[np.ndarray]:
+        """Measures every qubit of every instance in node order
+        (quantum_annealer.py:137-141 with bp_quantum_emulator.py:215-233):
+        round i measures node i of every instance that has one, all at once --
+        densities, outcome 0 when rho_00 > u, projector applied (apply1,
+        normalised), symmetric gauge, and a canonicalisation from random
+        messages of just the measured instances (per-instance stopping rule;
+        finished instances keep their state). ``samples`` (n_instances x
+        max nodes) gives the uniform draws, otherwise they are drawn on the
+        device from a generator seeded by ``seed``. Returns per instance the
+        configuration 1 - 2 * outcomes (the state ends projected)."""
+        L = self.layout
+        dev = L.device
+        sizes = [en.fields.shape[0] for en in self.energies]
+        nmax = max(sizes)
+        if samples is None:
+            gen = torch.Generator(device=dev).manual_seed(int(seed))
+            u_all = torch.rand((self.n_inst, nmax), generator=gen, dtype=torch.float64, device=dev)
+        else:
+            u_all = torch.as_tensor(np.asarray(samples, dtype=np.float64), device=dev)
+        outcomes = torch.zeros((self.n_inst, nmax), dtype=torch.int64, device=dev)
+        mp = _lib.MAX_PHYS
+        for i in range(nmax):
+            ks = [k for k in range(self.n_inst) if sizes[k] > i]
+            nodes = [self.node_idx[(k, i)] for k in ks]
+            nodes_dev = torch.as_tensor(nodes, dtype=torch.int32, device=dev)
+            kdev = torch.as_tensor(ks, device=dev)
+            # densities of the measured nodes (bp_quantum_emulator.py:188-207)
+            T = torch.empty_like(self.G)
+            _lib.call("dqz_symmetric_gauge", L.gptr, self.G.data_ptr(), self.lam.data_ptr(), EPS, T.data_ptr(),
+                      _lib.stream_handle())
+            n2e, e2n = L.new_msg_arena(), L.new_msg_arena()
+            _lib.call("dqz_lambdas_to_messages", L.gptr, self.lam.data_ptr(), n2e.data_ptr(), e2n.data_ptr(),
+                      L.max_chi(), _lib.stream_handle())
+            rho = density_packed(L, T, e2n, nodes)
+            r = (rho[:, 0, 0].real <= u_all[kdev, i]).to(torch.int64)
+            outcomes[kdev, i] = r
+            g = torch.zeros((len(nodes), mp * mp), dtype=torch.complex128, device=dev)
+            g[:, 0] = (1 - r).to(torch.complex128)
+            g[:, 3] = r.to(torch.complex128)
+            _lib.call("dqz_apply1", L.gptr, self.G.data_ptr(), nodes_dev.data_ptr(), g.data_ptr(), len(nodes),
+                      _lib.stream_handle())
+            T = torch.empty_like(self.G)
+            _lib.call("dqz_symmetric_gauge", L.gptr, self.G.data_ptr(), self.lam.data_ptr(), EPS, T.data_ptr(),
+                      _lib.stream_handle())
+            n2e, e2n = self._random_messages()
+            vd = torch.zeros(self.n_inst, dtype=torch.float64, device=dev)
+            vd[kdev] = np.finfo(np.float64).max
+            G = self.G.clone()
+            lam = self.lam.clone()
+            orth = torch.empty(max(L.msg_elems, 1), dtype=torch.complex128, device=dev)
+            partial = torch.zeros(max(L.n_halves, 1), dtype=torch.float64, device=dev)
+            self.G, self.lam = self._bp_loop(T, n2e, e2n, vd, G, lam, orth, partial)
+        out = outcomes.cpu().numpy()
+        return [1 - 2 * out[k, : sizes[k]] for k in range(self.n_inst)]
+
     def truncation_errors(self) -> List[np.ndarray]:
         """Per instance, in gate application order."""
         per = [[] for _ in range(self.n_inst)]

@@ -226,8 +226,13 @@ def run_quantum_annealer(
     synchronous_update: bool = False,
     traversal_type: str = "dfs",
     second_order: bool = False,
+    sample_measurements: bool = False,
+    samples: Optional[Sequence[float]] = None,
 ) -> QuantumAnnealingResults:
-    """Annealing on the BP emulator (quantum_annealer.py:90-152)."""
+    """Annealing on the BP emulator (quantum_annealer.py:90-152). With
+    ``sample_measurements`` every qubit is then measured in node order
+    (quantum_annealer.py:137-141) and ``configuration`` = 1 - 2 * outcomes;
+    ``samples`` (one uniform draw per qubit) replaces the emulator's own draws."""
     g = tensor_graph_of(energy)
     em = BPQuantumEmulator(g, key, max_chi, gates_number_per_regauging, accuracy,
                            max_belief_propagation_iterations, synchronous_update, traversal_type)
@@ -248,12 +253,17 @@ def run_quantum_annealer(
             em.apply_q1(mix, nid)
     rho = em.all_densities()
     order = [em._node_idx[i] for i in range(n)]
+    config = None
+    if sample_measurements:
+        outcomes = [em.measure(nid, None if samples is None else float(samples[nid])) for nid in range(n)]
+        config = 1 - 2 * np.array(outcomes, dtype=np.int64)
     return QuantumAnnealingResults(
         density_matrices=rho[order].cpu().numpy(),
         vidal_distances_after_regauging=em.after_regauging_vidal_distances.cpu().numpy(),
         truncation_affected_vidal_distances=em.truncated_affected_vidal_distances.cpu().numpy(),
         truncation_errors=np.array([float(x) for x in em.truncation_errors]),
         entropies=np.array([float(x) for x in em.entropies]),
+        configuration=config,
     )
 
 

@@ -125,3 +125,23 @@ def test_batched_annealer_equals_independent_runs():
                                      synchronous_update=True)
         assert np.abs(rho_b[k] - res.density_matrices).max() < 1e-9
         assert np.abs(errs_b[k] - res.truncation_errors).max() < 1e-9
+
+
+def test_batched_measurement_sampling_equals_independent_runs():
+    """Measuring every qubit after annealing (quantum_annealer.py:137-141):
+    the batched annealer, all instances per round, gives the same outcomes as
+    the emulator loop of each instance fed the same uniform draws."""
+    from dequantizer_b200.annealing import BatchedAnnealer
+
+    energies = [W.random_regular_energy(n, 3, seed=30 + n, field_std=0.5) for n in (8, 10)]
+    steps = list(W.scheduler(0.2, lambda t: 1 - t, 4))
+    U = np.random.default_rng(5).uniform(size=(2, 10))
+    ba = BatchedAnnealer(energies, max_chi=4, accuracy=1e-10, max_belief_propagation_iterations=200)
+    ba.run(steps)
+    configs = ba.sample_measurements(samples=U)
+    for k, en in enumerate(energies):
+        res = W.run_quantum_annealer(en, steps, key=1, max_chi=4, gates_number_per_regauging=en.edges_number,
+                                     accuracy=1e-10, max_belief_propagation_iterations=200,
+                                     synchronous_update=True, sample_measurements=True, samples=U[k])
+        assert np.array_equal(configs[k], res.configuration)
+        assert set(np.unique(configs[k])) <= {-1, 1}
