@@ -170,8 +170,8 @@ class AnnealingGradient:
             X = torch.stack([gam[v] for v in vs])
             X = torch.tensordot(X, G, dims=([X.dim() - 1], [1]))
             X = X / torch.linalg.vector_norm(X.reshape(len(vs), -1), dim=1).reshape((-1,) + (1,) * (X.dim() - 1))
-            for i, v in enumerate(vs):
-                out[v] = X[i]
+            for v, x in zip(vs, X.unbind(0)):  # unbind: one stack in the backward, not a select per item
+                out[v] = x
         return out
 
     def _prepare(self, X, others: List[torch.Tensor], half):
@@ -233,10 +233,11 @@ class AnnealingGradient:
         qb = finish(Wb, Pb, ob)
         gam = list(gam)
         lam = list(lam)
-        for i, g in enumerate(gts):
-            gam[g[1]] = torch.movedim(qa[i], qa.dim() - 2, g[2])
-            gam[g[3]] = torch.movedim(qb[i], qb.dim() - 2, g[4])
-            lam[g[0]] = lmbd[i, :rank]
+        lk = lmbd[:, :rank]
+        for g, xa, xb, l in zip(gts, qa.unbind(0), qb.unbind(0), lk.unbind(0)):
+            gam[g[1]] = torch.movedim(xa, xa.dim() - 1, g[2])  # (others.., d, rank): rank to the bond slot
+            gam[g[3]] = torch.movedim(xb, xb.dim() - 1, g[4])
+            lam[g[0]] = l
         return gam, lam
 
     def coupling_layer(self, gam, lam, tau):
@@ -287,8 +288,8 @@ class AnnealingGradient:
                 sh[f + 1] = Lf.shape[1]
                 X = X * Lf.reshape(sh).to(X.dtype)
             X = X / torch.linalg.vector_norm(X.reshape(len(vs), -1), dim=1).reshape((-1,) + (1,) * (nd - 1))
-            for i, v in enumerate(vs):
-                Ts[v] = X[i]
+            for v, x in zip(vs, X.unbind(0)):
+                Ts[v] = x
         T_arena = torch.cat([T.reshape(-1) for T in Ts])
         with torch.no_grad():
             n2e0 = torch.zeros(max(L.msg_elems, 1), dtype=torch.complex128, device=self.device)
@@ -306,18 +307,31 @@ class AnnealingGradient:
         else:
             n2e, _, _ = P.converge(T_arena, n2e0, self.bp_tol, self.bp_max)
         self.last_bp_sweeps.append(P.last_sweeps)
-        msgs = P.messages(n2e)
+        chi_groups = self._groups([int(l.shape[0]) for l in lam])
+        if len(chi_groups) == 1 and L.exact() and L.n_halves:
+            # one gather of both ends of every edge (a view per half-edge would
+            # give each its own full-arena gradient in the reverse pass)
+            c = next(iter(chi_groups))
+            per_half = n2e[: L.n_halves * c * c].view(L.n_halves, c, c)
+            msgs = None
+        else:
+            msgs = P.messages(n2e)
         orth: Dict[Tuple[int, int], torch.Tensor] = {}
         new_lam: List = [None] * len(self.edges)
-        for c, es in self._groups([int(l.shape[0]) for l in lam]).items():
+        for c, es in chi_groups.items():
             ends = [self.edge_ends[e] for e in es]
-            mf = torch.stack([msgs[int(L.node_half[a]) + ia] for a, ia, _, _ in ends])
-            mb = torch.stack([msgs[int(L.node_half[b]) + ib] for _, _, b, ib in ends])
+            if msgs is None:
+                hf = torch.as_tensor([int(L.node_half[a]) + ia for a, ia, _, _ in ends], device=self.device)
+                hb = torch.as_tensor([int(L.node_half[b]) + ib for _, _, b, ib in ends], device=self.device)
+                mf, mb = per_half[hf], per_half[hb]
+            else:
+                mf = torch.stack([msgs[int(L.node_half[a]) + ia] for a, ia, _, _ in ends])
+                mb = torch.stack([msgs[int(L.node_half[b]) + ib] for _, _, b, ib in ends])
             Gf, Gb, lb = self._edge_svd(mf, mb)
-            for i, (e, (a, ia, b, ib)) in enumerate(zip(es, ends)):
-                orth[(a, ia)] = Gf[i]
-                orth[(b, ib)] = Gb[i]
-                new_lam[e] = lb[i]
+            for e, (a, ia, b, ib), gf, gb, l in zip(es, ends, Gf.unbind(0), Gb.unbind(0), lb.unbind(0)):
+                orth[(a, ia)] = gf
+                orth[(b, ib)] = gb
+                new_lam[e] = l
         new_gam: List = [None] * N
         for shape, vs in node_groups.items():
             X = torch.stack([Ts[v] for v in vs])
@@ -328,8 +342,8 @@ class AnnealingGradient:
             spec = "n" + ax + "s," + ",".join("n" + ax[f] + out[f] for f in range(nb)) + "->n" + out + "s"
             X = torch.einsum(spec, *ops)
             X = X / torch.linalg.vector_norm(X.reshape(len(vs), -1), dim=1).reshape((-1,) + (1,) * (nb + 1))
-            for i, v in enumerate(vs):
-                new_gam[v] = X[i]
+            for v, x in zip(vs, X.unbind(0)):
+                new_gam[v] = x
         return new_gam, new_lam
 
     def _edge_svd(self, mf, mb):
