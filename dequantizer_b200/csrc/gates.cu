@@ -268,13 +268,19 @@ __global__ void __launch_bounds__(GATE_THREADS) simple_update_kernel(
     }
     __syncthreads();
     hestenes(core, zr, zr, kk, W, kk, sv, flag, red);
-    // unit columns of Z; null ones completed below
+    sort_desc(sv, kk, perm);
+    const int rank = (max_rank > 0 && max_rank < kk) ? max_rank : kk;
+    // unit columns of Z; null ones among the `rank` kept are completed below
+    // (the others are never read: they stay zero and count as accepted)
     for (int idx = threadIdx.x; idx < zr * kk; idx += blockDim.x) {
       const int c = idx / zr;
       const double sc = sv[c];
       core[idx] = sc > 1e-300 ? cscale(core[idx], 1.0 / sc) : czero();
     }
-    for (int c = threadIdx.x; c < kk; c += blockDim.x) acc[c] = sv[c] > 1e-300 ? 1 : 0;
+    for (int p = threadIdx.x; p < kk; p += blockDim.x) {
+      const int c = perm[p];
+      acc[c] = (sv[c] > 1e-300 || p >= rank) ? 1 : 0;
+    }
     __syncthreads();
     complete_orthonormal(core, zr, zr, kk, acc);
     // U columns: tall -> core (mu rows); else W (mu rows).
@@ -282,8 +288,6 @@ __global__ void __launch_bounds__(GATE_THREADS) simple_update_kernel(
     const cd *Ub = tall ? core : W;
     const cd *Vb = tall ? W : core;
     const int ldu = tall ? mu : kk, ldv = tall ? kk : mv;
-    sort_desc(sv, kk, perm);
-    const int rank = (max_rank > 0 && max_rank < kk) ? max_rank : kk;
     double n2 = 0.0;
     for (int c = threadIdx.x; c < kk; c += blockDim.x) {
       const double l = safe_truncate(sv[perm[c]], eps);

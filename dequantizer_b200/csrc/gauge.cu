@@ -3,8 +3,8 @@
 //                      chi <= 16, one CTA per edge above
 //  * absorb         -- tensor_ops.py:88-93 (absorb_by_node), one CTA per node
 //  * vidal_distance -- tensor_ops.py:143-175 + mappings/vidal_distance.py:17-42:
-//                      one warp per half-edge for chi <= 16 and bond slices of
-//                      <= 1024 entries, one CTA per half-edge above
+//                      one warp per half-edge for chi <= 16, one CTA per
+//                      half-edge above
 // vidal_edges, absorb and vidal_distance take an optional list of the
 // edges / nodes / half-edges to process (null = all).
 //  * symmetric      -- tensor_ops.py:189-199 (canonicalize)
@@ -19,7 +19,6 @@ namespace {
 constexpr int GAUGE_THREADS = 256;
 constexpr size_t SMEM_LIMIT = 200 * 1024;
 constexpr int WARP_MAX_CHI = 16;     // largest bond of the one-warp kernels
-constexpr int WARP_MAX_SLICE = 1024; // largest bond slice (size / chi) of the one-warp distance kernel
 constexpr int WARP_ROTS = 17;        // rotation slots per warp (n / 2 + 1 for n <= 32)
 constexpr size_t WARP_BLOCK_SMEM = 96 * 1024;
 constexpr int SCRATCH_GRID = 148 * 4;
@@ -369,27 +368,35 @@ __global__ void __launch_bounds__(GAUGE_THREADS) vidal_distance_kernel(dqz_graph
   }
 }
 
-// One warp per half-edge (chi <= WARP_MAX_CHI, bond slice <= max_slice <=
-// WARP_MAX_SLICE): the lambda^2 weight of every slice entry is formed once in
-// shared memory, each lane accumulates entries (a', a >= a') of R over the
-// slice, and the trace norm comes from warp_herm_eigh.
-__host__ __device__ inline size_t warp_vd_bytes(int c, int max_slice) {
+// One warp per half-edge (chi <= WARP_MAX_CHI). The bond slice is streamed
+// through the warp's shared memory in chunks of VD_CHUNK rows as
+// Y[x][a] = T[.., a@e, ..](x) * prod_{f != e} lambda_f[idx_f(x)], so that
+// R = Y^H Y (the lambda^2-weighted reduced matrix) reads every tensor entry
+// from L2 once; each lane accumulates up to VD_PAIRS entries (a' <= a) of R
+// from the staged rows, and the trace norm comes from warp_herm_eigh.
+constexpr int VD_CHUNK = 32;
+constexpr int VD_PAIRS = (WARP_MAX_CHI * (WARP_MAX_CHI + 1) / 2 + 31) / 32;
+
+__host__ __device__ inline size_t warp_vd_bytes(int c) {
   return round16(WARP_ROTS * sizeof(Rot)) + round16((size_t)c * c * sizeof(cd)) + round16((size_t)c * sizeof(double)) +
-         round16((size_t)max_slice * sizeof(double));
+         round16(VD_CHUNK * sizeof(double)) + round16((size_t)VD_CHUNK * c * sizeof(cd));
 }
 
-__global__ void __launch_bounds__(GAUGE_THREADS) vidal_distance_warp_kernel(
+__global__ void __launch_bounds__(GAUGE_THREADS, 3) vidal_distance_warp_kernel(
     dqz_graph_t g, const cd *__restrict__ Tall, const double *__restrict__ lambdas, double eps, double *partial,
-    int max_chi, int max_slice, const int32_t *__restrict__ sel, int n_sel) {
+    int max_chi, const int32_t *__restrict__ sel, int n_sel) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, wpb = blockDim.x >> 5;
-  unsigned char *wbase = smem_raw + (size_t)wid * warp_vd_bytes(max_chi, max_slice);
+  unsigned char *wbase = smem_raw + (size_t)wid * warp_vd_bytes(max_chi);
   Rot *rots = reinterpret_cast<Rot *>(wbase);
-  cd *Rm = reinterpret_cast<cd *>(wbase + round16(WARP_ROTS * sizeof(Rot)));
-  double *wv = reinterpret_cast<double *>(reinterpret_cast<unsigned char *>(Rm) +
-                                          round16((size_t)max_chi * max_chi * sizeof(cd)));
-  double *wx = reinterpret_cast<double *>(reinterpret_cast<unsigned char *>(wv) +
-                                          round16((size_t)max_chi * sizeof(double)));
+  unsigned char *q = wbase + round16(WARP_ROTS * sizeof(Rot));
+  cd *Rm = reinterpret_cast<cd *>(q);
+  q += round16((size_t)max_chi * max_chi * sizeof(cd));
+  double *wv = reinterpret_cast<double *>(q);
+  q += round16((size_t)max_chi * sizeof(double));
+  double *wl = reinterpret_cast<double *>(q);
+  q += round16(VD_CHUNK * sizeof(double));
+  cd *Ys = reinterpret_cast<cd *>(q);
   const int total = sel ? n_sel : g.n_halves;
   for (int it = blockIdx.x * wpb + wid; it < total; it += gridDim.x * wpb) {
     const int h = sel ? sel[it] : it;
@@ -398,45 +405,65 @@ __global__ void __launch_bounds__(GAUGE_THREADS) vidal_distance_warp_kernel(
     load_shape(g, v, s);
     const int e = h - s.half0;
     const int ce = s.dims[e];
-    const long long P64 = s.size / ce;
-    if (ce > max_chi || P64 > max_slice) {  // outside the caller's bounds: flag it
+    if (ce > max_chi || s.size >= (1ll << 31)) {  // outside the caller's bounds: flag it
       if (lane == 0) partial[h] = __longlong_as_double(0x7ff8000000000000ll);
       continue;
     }
-    const int P = (int)P64, Re = (int)s.stride[e];
+    const int P = (int)(s.size / ce), Re = (int)s.stride[e];
     const cd *T = Tall + g.node_off[v];
-    for (int x = lane; x < P; x += 32) {
-      const int l = x / Re, r = x - l * Re;
-      const int o0 = l * ce * Re + r;  // offset with a_e = 0
-      double wt = 1.0;
-      for (int f = 0; f < s.k; ++f) {
-        if (f == e) continue;
-        const int idx = (o0 / (int)s.stride[f]) % s.dims[f];
-        const double lv = lambdas[g.edge_lam_off[g.half_edge[s.half0 + f]] + idx];
-        wt *= lv * lv;
-      }
-      wx[x] = wt;
-    }
-    __syncwarp();
     const int npair = ce * (ce + 1) / 2;
-    const int nblk = P / Re;
-    for (int pi = lane; pi < npair; pi += 32) {
-      int ap = 0, rem = pi;
-      while (rem >= ce - ap) {
-        rem -= ce - ap;
-        ++ap;
+    int pa[VD_PAIRS], pb[VD_PAIRS];
+    cd acc[VD_PAIRS];
+#pragma unroll
+    for (int j = 0; j < VD_PAIRS; ++j) {
+      const int pi = lane + 32 * j;
+      pa[j] = -1;
+      pb[j] = 0;
+      acc[j] = czero();
+      if (pi < npair) {
+        int ap = 0, rem = pi;
+        while (rem >= ce - ap) {
+          rem -= ce - ap;
+          ++ap;
+        }
+        pa[j] = ap;
+        pb[j] = ap + rem;
       }
-      const int a = ap + rem;
-      const cd *Tp = T + (long long)ap * Re, *Ta = T + (long long)a * Re;
-      cd acc = czero();
-      int x = 0;
-      for (int l = 0; l < nblk; ++l) {
-        const int o = l * ce * Re;
-        for (int r = 0; r < Re; ++r, ++x) cfmac(acc, Tp[o + r], cscale(Ta[o + r], wx[x]));
-      }
-      Rm[ap * ce + a] = acc;
-      Rm[a * ce + ap] = cconj(acc);
     }
+    for (int x0 = 0; x0 < P; x0 += VD_CHUNK) {
+      const int nx = P - x0 < VD_CHUNK ? P - x0 : VD_CHUNK;
+      if (lane < nx) {  // lambda weight (not squared) of row x0 + lane
+        const int x = x0 + lane, l = x / Re, r = x - l * Re;
+        const int o0 = l * ce * Re + r;  // offset with a_e = 0
+        double wt = 1.0;
+        for (int f = 0; f < s.k; ++f) {
+          if (f == e) continue;
+          const int idx = (o0 / (int)s.stride[f]) % s.dims[f];
+          wt *= lambdas[g.edge_lam_off[g.half_edge[s.half0 + f]] + idx];
+        }
+        wl[lane] = wt;
+      }
+      __syncwarp();
+      for (int t = lane; t < nx * ce; t += 32) {  // rows x fastest across lanes
+        const int a = t / nx, jx = t - a * nx;
+        const int x = x0 + jx, l = x / Re, r = x - l * Re;
+        Ys[jx * ce + a] = cscale(T[(long long)(l * ce + a) * Re + r], wl[jx]);
+      }
+      __syncwarp();
+      for (int jx = 0; jx < nx; ++jx) {
+        const cd *row = Ys + jx * ce;
+#pragma unroll
+        for (int j = 0; j < VD_PAIRS; ++j)
+          if (pa[j] >= 0) cfmac(acc[j], row[pa[j]], row[pb[j]]);
+      }
+      __syncwarp();
+    }
+#pragma unroll
+    for (int j = 0; j < VD_PAIRS; ++j)
+      if (pa[j] >= 0) {
+        Rm[pa[j] * ce + pb[j]] = acc[j];
+        Rm[pb[j] * ce + pa[j]] = cconj(acc[j]);
+      }
     __syncwarp();
     cd tr = czero();
     for (int i = 0; i < ce; ++i) tr = cadd(tr, Rm[i * ce + i]);
@@ -640,16 +667,15 @@ extern "C" int dqz_vidal_distance(const dqz_graph_t *g, const void *tensors, con
   if (halves && (n_sel < 0 || n_sel > nh)) return DQZ_ERR_ARG;
   const int total = halves ? n_sel : nh;
   if (total > 0) {
-    if (max_chi <= WARP_MAX_CHI && max_slice > 0 && max_slice <= WARP_MAX_SLICE &&
-        dqz_get_tuning(DQZ_TUNE_GAUGE_PATH) != 2) {
-      const size_t per = warp_vd_bytes(max_chi, max_slice);
+    if (max_chi <= WARP_MAX_CHI && dqz_get_tuning(DQZ_TUNE_GAUGE_PATH) != 2) {
+      const size_t per = warp_vd_bytes(max_chi);
       int wpb = (int)(WARP_BLOCK_SMEM / per);
       wpb = wpb < 1 ? 1 : (wpb > GAUGE_THREADS / 32 ? GAUGE_THREADS / 32 : wpb);
       const int tuned = dqz_get_tuning(DQZ_TUNE_GAUGE_DIST_WARPS);
       if (tuned > 0 && (size_t)tuned * per <= SMEM_LIMIT) wpb = tuned;
       DQZ_SMEM_ATTR_ONCE(vidal_distance_warp_kernel, SMEM_LIMIT);
       vidal_distance_warp_kernel<<<(total + wpb - 1) / wpb, 32 * wpb, wpb * per, stream>>>(
-          *g, (const cd *)tensors, lambdas, eps, partial, max_chi, max_slice, halves, total);
+          *g, (const cd *)tensors, lambdas, eps, partial, max_chi, halves, total);
     } else {
       size_t smem = eigh_smem(max_chi) + 2 * (size_t)max_chi * max_chi * sizeof(cd) + (size_t)max_chi * sizeof(double);
       DQZ_SMEM_ATTR_ONCE(vidal_distance_kernel, SMEM_LIMIT);

@@ -136,8 +136,9 @@ def test_symmetric_gauge_density_and_lambdas(case):
 
 @pytest.mark.parametrize("case", ["small_bonds", "wide_slice", "large_bonds"])
 def test_vidal_distance_matches_oracle(case):
-    """small bonds: one warp per half-edge; a bond slice above 1024 entries
-    (degree 4, chi 12) or bonds above 16 (chi 20): one CTA per half-edge."""
+    """small bonds and a wide bond slice (degree 4, chi 12: 3456-row slices
+    streamed in chunks): one warp per half-edge; bonds above 16 (chi 20): one
+    CTA per half-edge."""
     g = {"small_bonds": lambda: G.get_nd_lattice([3, 2, 2], 2, 3),
          "wide_slice": lambda: G.get_nd_lattice([3, 3], 2, 12),
          "large_bonds": lambda: G.get_random_regular_graph(6, 3, 2, 20, 3)}[case]()
