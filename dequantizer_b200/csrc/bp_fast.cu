@@ -268,6 +268,104 @@ int launch_k3(const dqz_graph_t *g, const void *T, const void *n2e_old, const vo
   return DQZ_OK;
 }
 
+// X <- X x_bond m in place for batch index w (the warp's slice of X is both
+// read and written; every lane finishes its reads before any lane stores).
+template <int CHI, int BOND, typename C>
+__device__ __forceinline__ void mode_product_inplace(C *X, const C *__restrict__ m, int w) {
+  typedef typename RealOf<C>::R R;
+  constexpr int RS = Pad<CHI>::RS, SS = Pad<CHI>::SS, MS = Pad<CHI>::MS;
+  R re[CHI / 8][CHI / 4], im[CHI / 8][CHI / 4];
+  if (BOND == 0) {
+    warp_tile<CHI, CHI, MS, 1, SS, 1, false>(m, X + w * RS, re, im);
+    __syncwarp();
+    store_tile<CHI, SS, 1>(X + w * RS, re, im);
+  } else if (BOND == 1) {
+    warp_tile<CHI, CHI, MS, 1, RS, 1, false>(m, X + w * SS, re, im);
+    __syncwarp();
+    store_tile<CHI, RS, 1>(X + w * SS, re, im);
+  } else {
+    warp_tile<CHI, CHI, RS, 1, 1, MS, false>(X + w * SS, m, re, im);
+    __syncwarp();
+    store_tile<CHI, RS, 1>(X + w * SS, re, im);
+  }
+}
+
+// Vidal-gauge absorption (tensor_ops.py:88-93, absorb_by_node) for degree-3
+// nodes with bonds of dimension CHI and physical dimension 2, complex128:
+//     T'[a'][b'][c'][s] = sum_{a,b,c} G0[a][a'] G1[b][b'] G2[c][c'] T[a][b][c][s]
+// (G_f = the orthogonaliser of the node's f-th half-edge, row-major), then
+// T' / ||T'||_F. One CTA of 2 * CHI warps per node: both physical slabs stay
+// in padded shared memory, warp (s, w) owns batch index w of slab s in each
+// of the three in-place mode products, and the norm is reduced from shared
+// memory before the single write.
+template <int CHI>
+__global__ void __launch_bounds__(64 * CHI) absorb_k3(dqz_graph_t g, const double2 *__restrict__ Tin,
+                                                      const double2 *__restrict__ orth, double2 *Tout,
+                                                      const int32_t *__restrict__ sel, int total, int *error_flag) {
+  typedef double2 C;
+  constexpr int S2 = CHI * CHI, S3 = CHI * S2;
+  constexpr int RS = Pad<CHI>::RS, SS = Pad<CHI>::SS, MS = Pad<CHI>::MS, SLAB = Pad<CHI>::SLAB;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C *sX = reinterpret_cast<C *>(smem_raw);  // two slabs
+  C *sM = sX + 2 * SLAB;                    // three transposed orthogonalisers, CHI * MS each
+  __shared__ double red[48];
+  const int warp = threadIdx.x >> 5;
+  C *mine = sX + (warp / CHI) * SLAB;
+  const int w = warp % CHI;
+  for (int item = blockIdx.x; item < total; item += gridDim.x) {
+    const int v = sel ? sel[item] : item;
+    const int h0 = g.node_half[v];
+    bool ok = g.node_degree[v] == 3 && g.node_phys[v] == 2;
+    for (int f = 0; f < 3 && ok; ++f) ok = g.edge_chi[g.half_edge[h0 + f]] == CHI;
+    if (!ok) {
+      if (threadIdx.x == 0) atomicExch(error_flag, 1);
+      continue;
+    }
+    for (int i = threadIdx.x; i < 3 * S2; i += blockDim.x) {
+      const int f = i / S2, a = (i / CHI) % CHI, j = i % CHI;
+      sM[f * CHI * MS + j * MS + a] = orth[g.half_msg_off[h0 + f] + a * CHI + j];
+    }
+    const C *T = Tin + g.node_off[v];
+    for (int i = threadIdx.x; i < 2 * S3; i += blockDim.x) {
+      const int t = i >> 1;
+      sX[(i & 1) * SLAB + (t / S2) * SS + ((t / CHI) % CHI) * RS + t % CHI] = T[i];
+    }
+    __syncthreads();
+    mode_product_inplace<CHI, 0>(mine, sM, w);
+    __syncthreads();
+    mode_product_inplace<CHI, 1>(mine, sM + CHI * MS, w);
+    __syncthreads();
+    mode_product_inplace<CHI, 2>(mine, sM + 2 * CHI * MS, w);
+    __syncthreads();
+    double n2 = 0.0;
+    for (int i = threadIdx.x; i < 2 * S3; i += blockDim.x) {
+      const int t = i >> 1;
+      const C x = sX[(i & 1) * SLAB + (t / S2) * SS + ((t / CHI) % CHI) * RS + t % CHI];
+      n2 += x.x * x.x + x.y * x.y;
+    }
+    const double inv = 1.0 / sqrt(block_sum(n2, red));
+    C *O = Tout + g.node_off[v];
+    for (int i = threadIdx.x; i < 2 * S3; i += blockDim.x) {
+      const int t = i >> 1;
+      const C x = sX[(i & 1) * SLAB + (t / S2) * SS + ((t / CHI) % CHI) * RS + t % CHI];
+      O[i] = make_double2(x.x * inv, x.y * inv);
+    }
+    __syncthreads();
+  }
+}
+
+template <int CHI>
+int launch_absorb_k3(const dqz_graph_t *g, const void *tin, const void *orth, void *tout, const int32_t *sel,
+                     int total, int *error_flag, cudaStream_t stream) {
+  const size_t smem = (2 * (size_t)Pad<CHI>::SLAB + 3 * (size_t)CHI * Pad<CHI>::MS) * sizeof(double2);
+  if (smem > 227 * 1024) return DQZ_ERR_UNSUPPORTED;
+  DQZ_SMEM_ATTR_ONCE(absorb_k3<CHI>, smem);
+  absorb_k3<CHI><<<total, 64 * CHI, smem, stream>>>(*g, (const double2 *)tin, (const double2 *)orth,
+                                                     (double2 *)tout, sel, total, error_flag);
+  DQZ_CHECK_LAUNCH();
+  return DQZ_OK;
+}
+
 template <typename W>
 __global__ void edge_pass_words(dqz_graph_t g, const W *n2e_old, const W *n2e_new, const uint8_t *edge_new,
                                 W *e2n_new) {
@@ -302,6 +400,18 @@ extern "C" int dqz_bp_node_update_k3(const dqz_graph_t *g, int32_t chi, int32_t 
     if (chi == 8) return launch_k3<8, float2>(g, tensors, n2e_old, e2n_old, n2e_new, src_sel, halves, n_halves,
                                               error_flag, stream);
   }
+  return DQZ_ERR_UNSUPPORTED;
+}
+
+extern "C" int dqz_absorb_k3(const dqz_graph_t *g, int32_t chi, const void *tensors_in, const void *orth,
+                             void *tensors_out, const int32_t *nodes, int32_t n_sel, int32_t *error_flag,
+                             cudaStream_t stream) {
+  if (!g || !tensors_in || !orth || !tensors_out || !error_flag) return DQZ_ERR_ARG;
+  if (nodes && (n_sel < 0 || n_sel > g->n_nodes)) return DQZ_ERR_ARG;
+  const int total = nodes ? n_sel : g->n_nodes;
+  if (total == 0) return DQZ_OK;
+  if (chi == 16) return launch_absorb_k3<16>(g, tensors_in, orth, tensors_out, nodes, total, error_flag, stream);
+  if (chi == 8) return launch_absorb_k3<8>(g, tensors_in, orth, tensors_out, nodes, total, error_flag, stream);
   return DQZ_ERR_UNSUPPORTED;
 }
 

@@ -302,8 +302,13 @@ def vidal_gauge_packed(layout: GraphLayout, T, n2e, eps: float, out=None, edges=
     scratch = _scratch(nb, layout.device) if nb else None
     _lib.call("dqz_vidal_edges", layout.gptr, n2e.data_ptr(), float(eps), orth.data_ptr(), lam.data_ptr(), max_chi,
               _lib.ptr(edges), ne if edges is not None else 0, _lib.ptr(scratch), stream)
-    ms = layout.max_size()
     nn = layout.n_nodes if nodes is None else int(nodes.numel())
+    chi3 = layout.uniform_k3_chi()
+    if chi3:
+        _lib.call("dqz_absorb_k3", layout.gptr, chi3, T.data_ptr(), orth.data_ptr(), G.data_ptr(), _lib.ptr(nodes),
+                  nn if nodes is not None else 0, error_flag(layout.device).data_ptr(), stream)
+        return G, lam
+    ms = layout.max_size()
     nb = _lib.lib().dqz_absorb_scratch_bytes(nn, ms)
     scratch = _scratch(nb, layout.device) if nb else None
     _lib.call("dqz_absorb", layout.gptr, T.data_ptr(), orth.data_ptr(), G.data_ptr(), ms, _lib.ptr(nodes),

@@ -208,6 +208,13 @@ size_t dqz_vidal_edges_scratch_bytes(int32_t n_edges, int32_t max_chi);
 int dqz_absorb(const dqz_graph_t *g, const void *tensors_in, const void *orth, void *tensors_out,
                int32_t max_size, const int32_t *nodes, int32_t n_sel, void *scratch, cudaStream_t stream);
 size_t dqz_absorb_scratch_bytes(int32_t n_nodes, int32_t max_size);
+/* The same for degree-3 nodes with physical dimension 2 and every bond of
+ * dimension chi (8 or 16), one CTA per node with the tensor held in shared
+ * memory; needs no scratch. A node of any other shape is skipped and sets
+ * *error_flag (device int) to 1. */
+int dqz_absorb_k3(const dqz_graph_t *g, int32_t chi, const void *tensors_in, const void *orth,
+                  void *tensors_out, const int32_t *nodes, int32_t n_sel, int32_t *error_flag,
+                  cudaStream_t stream);
 
 /* ---- Vidal distance (mappings/vidal_distance.py:17-42, tensor_ops.py:143-175)
  * partial[h] = trace norm for half-edge h; out (optional, NULL to skip) =

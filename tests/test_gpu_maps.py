@@ -218,6 +218,56 @@ def test_gauge_selection_updates_only_listed_entries():
     assert np.all(p[~mask] == -1.0)
 
 
+@pytest.mark.parametrize("chi", [8, 16])
+def test_degree3_absorb_matches_generic_and_oracle(chi):
+    """dqz_absorb_k3 (shared-memory degree-3 form) against the generic
+    dqz_absorb and the oracle's absorb_by_node on arbitrary (non-orthogonal)
+    bond matrices; with a node list it writes only the listed nodes."""
+    from dequantizer_b200 import _lib
+    from dequantizer_b200.layout import GraphLayout
+
+    g = G.get_random_regular_graph(12, 3, 2, chi, 5)
+    tensors = random_tensors(g, 9)
+    trav, _ = _converged_messages(g, tensors, n=1)
+    topo = M.Topology(trav, True)
+    L = GraphLayout(topo.nodes, topo.edges, [e.dimension for e in topo.edges])
+    assert L.uniform_k3_chi() == chi
+    T = L.pack_tensors([torch.from_numpy(tensors[n.id]).cuda() for n in topo.nodes])
+    rng = np.random.default_rng(chi)
+    mats = [rng.standard_normal((chi, chi)) + 1j * rng.standard_normal((chi, chi)) for _ in range(L.n_halves)]
+    orth = L.pack_messages([torch.from_numpy(m).cuda() for m in mats])
+    stream = _lib.stream_handle()
+    flag = torch.zeros(1, dtype=torch.int32, device=T.device)
+    G_k3 = torch.full_like(T, 7.0)
+    _lib.call("dqz_absorb_k3", L.gptr, chi, T.data_ptr(), orth.data_ptr(), G_k3.data_ptr(), None, 0,
+              flag.data_ptr(), stream)
+    ms = L.max_size()
+    nb = _lib.lib().dqz_absorb_scratch_bytes(L.n_nodes, ms)
+    scratch = torch.empty(max(nb, 1), dtype=torch.uint8, device=T.device)
+    G_gen = torch.full_like(T, 7.0)
+    _lib.call("dqz_absorb", L.gptr, T.data_ptr(), orth.data_ptr(), G_gen.data_ptr(), ms, None, 0,
+              scratch.data_ptr(), stream)
+    torch.cuda.synchronize()
+    assert int(flag.item()) == 0
+    assert float((G_k3 - G_gen).abs().max()) < 1e-13
+    sizes = L.node_sizes()
+    for v, node in enumerate(topo.nodes):
+        o, n = int(L.node_off[v]), int(sizes[v])
+        ref = OT.absorb_by_node(tensors[node.id], [mats[int(L.node_half[v]) + f] for f in range(3)])
+        assert rel_err(G_k3[o:o + n].reshape(ref.shape), ref) < 1e-13
+    nodes = torch.tensor([1, 4, 5, 10], dtype=torch.int32, device=T.device)
+    G_sel = torch.full_like(T, 7.0)
+    _lib.call("dqz_absorb_k3", L.gptr, chi, T.data_ptr(), orth.data_ptr(), G_sel.data_ptr(), nodes.data_ptr(),
+              int(nodes.numel()), flag.data_ptr(), stream)
+    torch.cuda.synchronize()
+    for v in range(L.n_nodes):
+        o, n = int(L.node_off[v]), int(sizes[v])
+        if v in (1, 4, 5, 10):
+            assert torch.equal(G_sel[o:o + n], G_k3[o:o + n])
+        else:
+            assert bool((G_sel[o:o + n] == 7.0).all())
+
+
 def test_apply1_apply2_match_oracle():
     g_ref = G.get_nd_lattice([2, 3], 2, 2)
     g_gpu = G.get_nd_lattice([2, 3], 2, 2)
