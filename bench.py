@@ -233,6 +233,7 @@ NCU_TRAFFIC = {
     ("bp_node_k3", "fp64"): 158.0e6,
     ("bp_node_k3", "fp32"): 77.6e6,
     ("bp_node_k3_tc", "bf16"): 39.9e6,
+    ("bp_node_k3_umma", "bf16"): 75.0e6,
 }
 
 

@@ -82,6 +82,9 @@ _SIGNATURES = {
     "dqz_bp_node_update_k3": (ctypes.c_int, [_G, _I, _I, _P, _P, _P, _P, _P, _P, _I, _P, _P]),
     "dqz_bp_edge_pass_c64": (ctypes.c_int, [_G, _P, _P, _P, _P, _P]),
     "dqz_bp_node_update_k3_tc": (ctypes.c_int, [_G, _P, _P, _P, _P, _P, _P, _I, _P, _P]),
+    "dqz_bp_node_update_k3_umma": (ctypes.c_int, [_G, _P, _P, _P, _P, _P, _P, _I, _P, _P]),
+    "dqz_bf16_umma_elems_per_node": (_S, []),
+    "dqz_pack_bf16_umma": (ctypes.c_int, [_G, _P, _P, _P]),
     "dqz_pack_bf16_planes": (ctypes.c_int, [_G, _P, _P, _P]),
     "dqz_messages_distance": (ctypes.c_int, [_G, _P, _P, _P, _P, _P, _P, _I, _P]),
     "dqz_reduce_sum": (ctypes.c_int, [_P, _I, _D, _P, _P]),

@@ -9,7 +9,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libdqz.so")
-SOURCES = ["capi.cu", "bp.cu", "bp_fast.cu", "bp_tc.cu", "gauge.cu", "gates.cu", "adjoint.cu", "qr.cu", "statevec.cu"]
+SOURCES = ["capi.cu", "bp.cu", "bp_fast.cu", "bp_tc.cu", "bp_umma.cu", "gauge.cu", "gates.cu", "adjoint.cu", "qr.cu", "statevec.cu"]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-O3", "-lineinfo", "-std=c++17",

@@ -106,7 +106,6 @@ __global__ void bp_edge_pass_kernel(dqz_graph_t g, const cd *n2e_old, const cd *
   const int nh = g.n_halves;
   // one warp per half-edge
   const int warps_per_block = blockDim.x >> 5;
-  const int lane = threadIdx.x & 31;
   for (int h = blockIdx.x * warps_per_block + (threadIdx.x >> 5); h < nh; h += gridDim.x * warps_per_block) {
     const int e = g.half_edge[h];
     const int tw = g.half_twin[h];
@@ -114,7 +113,7 @@ __global__ void bp_edge_pass_kernel(dqz_graph_t g, const cd *n2e_old, const cd *
     const int c = g.edge_chi[e];
     const cd *src = (edge_new[h] ? n2e_new : n2e_old) + g.half_msg_off[tw];
     cd *dst = e2n_new + g.half_msg_off[h];
-    for (int i = lane; i < c * c; i += 32) dst[i] = src[i];
+    warp_copy16(reinterpret_cast<uint4 *>(dst), reinterpret_cast<const uint4 *>(src), c * c);
   }
 }
 

@@ -376,7 +376,11 @@ __global__ void edge_pass_words(dqz_graph_t g, const W *n2e_old, const W *n2e_ne
     const int c = g.edge_chi[e];
     const W *src = (edge_new[h] ? n2e_new : n2e_old) + g.half_msg_off[tw];
     W *dst = e2n_new + g.half_msg_off[h];
-    for (int i = lane; i < c * c; i += 32) dst[i] = src[i];
+    const int bytes = c * c * (int)sizeof(W);
+    if (bytes % 16 == 0 && ((reinterpret_cast<uintptr_t>(src) | reinterpret_cast<uintptr_t>(dst)) & 15) == 0)
+      warp_copy16(reinterpret_cast<uint4 *>(dst), reinterpret_cast<const uint4 *>(src), bytes / 16);
+    else
+      for (int i = lane; i < c * c; i += 32) dst[i] = src[i];
   }
 }
 

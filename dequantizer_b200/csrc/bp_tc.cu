@@ -22,6 +22,7 @@
 #include <cuda_bf16.h>
 
 #include "common.cuh"
+#include "mma_bf16.cuh"
 
 namespace {
 
@@ -43,32 +44,6 @@ struct __align__(16) TcSmem {
   float red[2];
 };
 static_assert(sizeof(float) * 8 * 2 * 2 * 32 * 4 <= sizeof(__nv_bfloat16) * 2 * NAT, "partials fit in X");
-
-__device__ __forceinline__ uint32_t saddr(const void *p) { return static_cast<uint32_t>(__cvta_generic_to_shared(p)); }
-
-__device__ __forceinline__ void ldsm_x4(uint32_t addr, uint32_t &r0, uint32_t &r1, uint32_t &r2, uint32_t &r3) {
-  asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
-               : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3)
-               : "r"(addr));
-}
-__device__ __forceinline__ void ldsm_x4_t(uint32_t addr, uint32_t &r0, uint32_t &r1, uint32_t &r2, uint32_t &r3) {
-  asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0,%1,%2,%3}, [%4];\n"
-               : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3)
-               : "r"(addr));
-}
-
-__device__ __forceinline__ void mma_bf16(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
-  asm volatile(
-      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
-      "{%0,%1,%2,%3};\n"
-      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
-}
-
-__device__ __forceinline__ void neg4(const uint32_t (&a)[4], uint32_t (&o)[4]) {
-#pragma unroll
-  for (int i = 0; i < 4; ++i) o[i] = a[i] ^ 0x80008000u;
-}
 
 // --- fragment loaders. For an A tile (16 m x 16 k) the four 8x8 matrices are
 // (m 0-7,k 0-7), (m 8-15,k 0-7), (m 0-7,k 8-15), (m 8-15,k 8-15); lane i
@@ -100,42 +75,6 @@ __device__ __forceinline__ void load_b_trans(const __nv_bfloat16 *base, int kstr
   const int lane = threadIdx.x & 31, j = lane >> 3;
   const __nv_bfloat16 *p = base + ((j & 1) * 8 + (lane & 7)) * kstride + (j >> 1) * 8;
   ldsm_x4_t(saddr(p), b[0][0], b[0][1], b[1][0], b[1][1]);
-}
-
-// Complex tile: D(16 x 16) += A * B, Dr += Ar Br - Ai Bi, Di += Ar Bi + Ai Br.
-__device__ __forceinline__ void cmma(const uint32_t (&ar)[4], const uint32_t (&ai)[4], const uint32_t (&br)[2][2],
-                                     const uint32_t (&bi)[2][2], float (&dr)[2][4], float (&di)[2][4]) {
-  uint32_t nai[4];
-  neg4(ai, nai);
-#pragma unroll
-  for (int nt = 0; nt < 2; ++nt) {
-    mma_bf16(dr[nt], ar, br[nt][0], br[nt][1]);
-    mma_bf16(dr[nt], nai, bi[nt][0], bi[nt][1]);
-    mma_bf16(di[nt], ar, bi[nt][0], bi[nt][1]);
-    mma_bf16(di[nt], ai, br[nt][0], br[nt][1]);
-  }
-}
-// Conjugated B: D += A * conj(B): Dr += Ar Br + Ai Bi, Di += Ai Br - Ar Bi.
-__device__ __forceinline__ void cmma_conjb(const uint32_t (&ar)[4], const uint32_t (&ai)[4],
-                                           const uint32_t (&br)[2][2], const uint32_t (&bi)[2][2],
-                                           float (&dr)[2][4], float (&di)[2][4]) {
-  uint32_t nar[4];
-  neg4(ar, nar);
-#pragma unroll
-  for (int nt = 0; nt < 2; ++nt) {
-    mma_bf16(dr[nt], ar, br[nt][0], br[nt][1]);
-    mma_bf16(dr[nt], ai, bi[nt][0], bi[nt][1]);
-    mma_bf16(di[nt], ai, br[nt][0], br[nt][1]);
-    mma_bf16(di[nt], nar, bi[nt][0], bi[nt][1]);
-  }
-}
-
-__device__ __forceinline__ const float2 *msg_c64(const dqz_graph_t &g, int hf, const float2 *n2e_old,
-                                                 const float2 *e2n_old, const float2 *n2e_new,
-                                                 const uint8_t *src_sel) {
-  const int sel = src_sel[hf];
-  if (sel == DQZ_SRC_E2N_OLD) return e2n_old + g.half_msg_off[hf];
-  return (sel == DQZ_SRC_N2E_NEW ? n2e_new : n2e_old) + g.half_msg_off[g.half_twin[hf]];
 }
 
 // D fragment element (row r, col c) of an m16n8 tile: held by lane

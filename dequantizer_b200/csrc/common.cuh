@@ -55,6 +55,26 @@ __device__ __forceinline__ cd warp_csum(cd v) {
   return v;
 }
 
+// Warp copy of n16 16-byte chunks between non-overlapping buffers: each lane
+// issues up to four loads before their stores, so a message costs one memory
+// round trip per 2 KB instead of one per element.
+__device__ __forceinline__ void warp_copy16(uint4 *__restrict__ dst, const uint4 *__restrict__ src, int n16) {
+  const int lane = threadIdx.x & 31;
+  for (int base = 0; base < n16; base += 128) {
+    uint4 buf[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int i = base + lane + 32 * j;
+      if (i < n16) buf[j] = src[i];
+    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int i = base + lane + 32 * j;
+      if (i < n16) dst[i] = buf[j];
+    }
+  }
+}
+
 // Sum over the CTA; every thread gets the result. `red` needs 33 doubles of
 // shared memory. Contains __syncthreads, so all threads must call it.
 __device__ __forceinline__ double block_sum(double v, double *red) {

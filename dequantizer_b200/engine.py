@@ -29,7 +29,7 @@ import torch
 from . import _lib
 from .graph import TensorGraph
 from .layout import GraphLayout
-from .maps import Topology, bp_sweep, density_packed, error_flag, vidal_distance_packed, vidal_gauge_packed
+from .maps import BF16_KERNELS, Topology, bp_sweep, density_packed, error_flag, vidal_distance_packed, vidal_gauge_packed
 
 SCHEDULES = ("sync", "async", "flooding")
 PRECISIONS = {"fp64": torch.complex128, "fp32": torch.complex64, "bf16": torch.complex64}
@@ -37,7 +37,7 @@ PRECISIONS = {"fp64": torch.complex128, "fp32": torch.complex64, "bf16": torch.c
 
 class BPEngine:
     def __init__(self, graph: TensorGraph, traversal: str = "dfs", schedule: str = "sync", precision: str = "fp64",
-                 device=None):
+                 device=None, bf16_kernel: str = "tcgen05"):
         if schedule not in SCHEDULES:
             raise ValueError(f"schedule must be one of {SCHEDULES}")
         if precision not in PRECISIONS:
@@ -64,9 +64,13 @@ class BPEngine:
         self._spare = (self._arena(L.msg_elems), self._arena(L.msg_elems))
         self._partial = torch.empty(max(2 * L.n_halves, 1), dtype=torch.float64, device=L.device)
         self._stage = {}
-        # bf16: node tensors also kept as BF16 planes (16384 per node), rebuilt
-        # from T after every load
-        self.T_bf16 = (torch.empty(L.n_nodes * 16384, dtype=torch.bfloat16, device=L.device)
+        # bf16: node tensors also kept in BF16, rebuilt from T after every
+        # load: the tcgen05 kernel's core layouts, or the mma_sync kernel's planes
+        if bf16_kernel not in BF16_KERNELS:
+            raise ValueError(f"bf16_kernel must be one of {tuple(BF16_KERNELS)}")
+        self.bf16_kernel = bf16_kernel
+        per_node = int(_lib.lib().dqz_bf16_umma_elems_per_node()) if bf16_kernel == "tcgen05" else 16384
+        self.T_bf16 = (torch.empty(L.n_nodes * per_node, dtype=torch.bfloat16, device=L.device)
                        if precision == "bf16" else None)
         self._bf16_stale = True
 
@@ -76,7 +80,7 @@ class BPEngine:
     @property
     def kernel(self) -> str:
         if self.precision == "bf16":
-            return "bp_node_k3_tc"
+            return "bp_node_k3_umma" if self.bf16_kernel == "tcgen05" else "bp_node_k3_tc"
         return "bp_node_k3" if self.layout.uniform_k3_chi() else "bp_node_generic"
 
     # -------------------------------------------------------------- load
@@ -130,11 +134,12 @@ class BPEngine:
         updates and the edge pass, to time the node-update kernel alone."""
         n2e_new, e2n_new = self._spare
         if self.T_bf16 is not None and self._bf16_stale:
-            _lib.call("dqz_pack_bf16_planes", self.layout.gptr, self.T.data_ptr(), self.T_bf16.data_ptr(),
+            pack = "dqz_pack_bf16_umma" if self.bf16_kernel == "tcgen05" else "dqz_pack_bf16_planes"
+            _lib.call(pack, self.layout.gptr, self.T.data_ptr(), self.T_bf16.data_ptr(),
                       _lib.stream_handle())
             self._bf16_stale = False
         bp_sweep(self.layout, self.topo, self.T, self.n2e, self.e2n, n2e_new, e2n_new, mid_event,
-                 T_bf16=self.T_bf16)
+                 T_bf16=self.T_bf16, bf16_kernel=self.bf16_kernel)
         self._spare = (self.n2e, self.e2n)
         self._prev = (self.n2e, self.e2n)
         self.n2e, self.e2n = n2e_new, e2n_new

@@ -172,16 +172,20 @@ def error_flag(device) -> torch.Tensor:
     return _ERROR_FLAGS[key]
 
 
+BF16_KERNELS = {"tcgen05": "dqz_bp_node_update_k3_umma", "mma_sync": "dqz_bp_node_update_k3_tc"}
+
+
 def bp_sweep(layout: GraphLayout, topo: Topology, T, n2e_old, e2n_old, n2e_new, e2n_new, mid_event=None,
-             T_bf16=None):
+             T_bf16=None, bf16_kernel: str = "tcgen05"):
     """One sweep on packed arenas: node updates level by level, then the edge pass
     (``mid_event``, a torch.cuda.Event, is recorded between the two).
 
     complex128 arenas use the specialised degree-3 kernel when every node
     has that shape (layout.uniform_k3_chi), the generic kernel otherwise;
     complex64 arenas need the specialised shape and run in FP32, or, when
-    ``T_bf16`` (BF16 planes from dqz_pack_bf16_planes) is given, as BF16
-    tensor-core products with FP32 accumulation (bonds of dimension 16)."""
+    ``T_bf16`` is given, as BF16 tensor-core products with FP32 accumulation
+    (bonds of dimension 16): ``bf16_kernel`` "tcgen05" takes the core layouts
+    of dqz_pack_bf16_umma, "mma_sync" the planes of dqz_pack_bf16_planes."""
     src_sel, edge_new, levels = topo.device_tables(layout.device)
     stream = _lib.stream_handle()
     chi3 = layout.uniform_k3_chi()
@@ -192,7 +196,7 @@ def bp_sweep(layout: GraphLayout, topo: Topology, T, n2e_old, e2n_old, n2e_new, 
         flag = error_flag(layout.device)
         if T_bf16 is not None:
             for nodes in topo.device_node_levels(layout.device):
-                _lib.call("dqz_bp_node_update_k3_tc", layout.gptr, T_bf16.data_ptr(), n2e_old.data_ptr(),
+                _lib.call(BF16_KERNELS[bf16_kernel], layout.gptr, T_bf16.data_ptr(), n2e_old.data_ptr(),
                           e2n_old.data_ptr(), n2e_new.data_ptr(), src_sel.data_ptr(), nodes.data_ptr(),
                           nodes.numel(), flag.data_ptr(), stream)
         else:

@@ -124,6 +124,21 @@ int dqz_bp_node_update_k3_tc(const dqz_graph_t *g, const void *tensors_bf16, con
 int dqz_pack_bf16_planes(const dqz_graph_t *g, const void *tensors_c64, void *tensors_bf16,
                          cudaStream_t stream);
 
+/* The same node update with the mode products on the 5th-generation tensor
+ * cores (tcgen05.mma, accumulators in tensor memory; the three final 16 x 16
+ * contractions as warp-level MMAs). `tensors_bf16` holds every node tensor as
+ * dqz_bf16_umma_elems_per_node() BF16 elements at v * that count, 16-byte
+ * aligned, built by dqz_pack_bf16_umma. A node of any other shape sets
+ * *error_flag to 1; a wait that runs out (no progress for seconds) sets it to 2. */
+int dqz_bp_node_update_k3_umma(const dqz_graph_t *g, const void *tensors_bf16, const void *n2e_old,
+                               const void *e2n_old, void *n2e_new, const uint8_t *src_sel,
+                               const int32_t *nodes, int32_t n_nodes, int32_t *error_flag,
+                               cudaStream_t stream);
+size_t dqz_bf16_umma_elems_per_node(void);
+/* complex64 node tensors (node_off layout) -> the BF16 core layouts above. */
+int dqz_pack_bf16_umma(const dqz_graph_t *g, const void *tensors_c64, void *tensors_bf16,
+                       cudaStream_t stream);
+
 /* Edge pass on complex64 messages (see dqz_bp_edge_pass). */
 int dqz_bp_edge_pass_c64(const dqz_graph_t *g, const void *n2e_old, const void *n2e_new,
                          const uint8_t *edge_new, void *e2n_new, cudaStream_t stream);

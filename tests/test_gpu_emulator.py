@@ -160,6 +160,33 @@ def test_engine_bf16_sweeps_track_fp64():
     engines["bf16"].check()
 
 
+@pytest.mark.parametrize("schedule", ["sync", "async"])
+def test_bf16_tcgen05_kernel_matches_mma_sync_kernel(schedule):
+    """The tcgen05 node update (mode products in tensor memory) and the
+    warp-MMA one round the same intermediates to BF16 and accumulate in FP32:
+    after one and after three sweeps from the same start their messages agree
+    to 1e-2 of the largest entry (FP32 summation order moves BF16 roundings),
+    both stay within 3e-2 of FP64, and no node is skipped."""
+    g, tensors, m = _bench_like(40, 11)
+    engines = {k: BPEngine(g, schedule=schedule, precision="bf16", bf16_kernel=k) for k in ("tcgen05", "mma_sync")}
+    ref = BPEngine(g, schedule=schedule, precision="fp64")
+    for e in list(engines.values()) + [ref]:
+        e.load_tensors(tensors)
+        e.load_messages([m] * e.layout.n_halves)
+    assert engines["tcgen05"].kernel == "bp_node_k3_umma"
+    for n_sweeps in (1, 2):
+        for e in list(engines.values()) + [ref]:
+            for _ in range(n_sweeps):
+                e.sweep()
+        a = engines["tcgen05"].n2e.to(torch.complex128)
+        b = engines["mma_sync"].n2e.to(torch.complex128)
+        assert bool(torch.isfinite(a).all())
+        assert float((a - b).abs().max() / b.abs().max()) < 1e-2
+        assert float((a - ref.n2e).abs().max() / ref.n2e.abs().max()) < 3e-2
+    for e in engines.values():
+        e.check()
+
+
 def test_engine_bf16_meets_z_bound_at_fixed_point():
     """<Z_i> after BP to the fixed point: BF16 sweeps vs FP64 sweeps,
     |delta <Z_i>| <= 1e-4 (the mixed-precision accuracy bound)."""
