@@ -543,11 +543,96 @@ def run_grad(args, world, rank, local):
         }), flush=True)
 
 
+def run_ising3d(args, world, rank, local):
+    """3-D Ising square-root network (examples/3d_ising_canonicalization.py:89-160):
+    6 x 6 x 6 open lattice, bond dimension 2, Potts tensors with J = -1 and field
+    h = 0.5 at beta = 0.1 ... 0.5; for each beta, asynchronous DFS sweeps from the
+    seeded non-negative messages, each followed by the Vidal gauge and the Vidal
+    distance, until that distance is <= 1e-10 (at most 500 sweeps). A step is one
+    scan over the five betas; the unit is BP iterations/s (sweep + gauge +
+    distance). Work is tiny (7.6 MFLOP per sweep) and launch / latency bound, so
+    no roofline fraction is reported. Ranks run replicas."""
+    import torch
+
+    from dequantizer_b200.workloads import ising_sqrt_partition
+
+    betas = [0.1, 0.2, 0.3, 0.4, 0.5]
+    kw = dict(lattice_sizes=[6, 6, 6], betas=betas, coupling=-1.0, field_strength=0.5, accuracy=1e-10,
+              open_boundary=True, synchronous_update=False, key=42, traversal_type="dfs", max_iterations=500)
+    for _ in range(args.warmup):
+        ising_sqrt_partition(**kw)
+    torch.cuda.synchronize()
+    barrier(world)
+    iters = 0
+    with ClockSampler(local) as clk:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            res = ising_sqrt_partition(**kw)
+            iters += sum(res.number_of_iterations)
+        e1.record()
+        e1.synchronize()
+    elapsed = reduce_max(e0.elapsed_time(e1) * 1e-3, world)
+    n_edges = 3 * 6 * 6 * 5
+    if rank == 0:
+        print(json.dumps({
+            "metric": METRIC, "workload": "3-D Ising canonicalisation", "value": world * iters / elapsed,
+            "unit": "BP iterations/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": elapsed / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+            "config": {"lattice": "6x6x6 open", "chi": 2, "d": 2, "coupling": -1.0, "field": 0.5,
+                       "betas": betas, "vidal_distance_tol": 1e-10, "max_sweeps": 500,
+                       "schedule": "asynchronous DFS sweep + Vidal gauge + Vidal distance per iteration"},
+            "iterations_per_scan": iters // max(args.steps, 1),
+            "edge_updates_per_s": world * iters * 2 * n_edges / elapsed,
+            "average_magnetization": res.average_magnetization, "roofline": None,
+            "clocks": clk.summary(),
+        }), flush=True)
+
+
+def run_eagle(args, world, rank, local):
+    """Kicked Ising on the 127-qubit heavy-hex lattice (examples/ibm_eagle_processor.py:56-145):
+    RX(0.6) on every qubit and RZZ(-pi/2) on every edge per Trotter step, the
+    RZZ gates in the three classes of a proper edge colouring with a Vidal
+    regauge (BP accuracy 1e-5) after each class, bond dimension up to 32,
+    <Z_i> of every qubit after each step. A step is one Trotter step; the
+    unit is Trotter steps/s. Ranks run replicas."""
+    import torch
+
+    from dequantizer_b200.workloads import run_eagle_simulation
+
+    n_steps = 20
+    torch.cuda.synchronize()
+    barrier(world)
+    with ClockSampler(local) as clk:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        z, em = run_eagle_simulation(max_chi=32, layers_per_regauging=1, trotter_steps=n_steps, accuracy=1e-5,
+                                     theta=0.6, is_infinite=False, colour_classes=True, all_qubits=True)
+        e1.record()
+        e1.synchronize()
+    elapsed = reduce_max(e0.elapsed_time(e1) * 1e-3, world)
+    if rank == 0:
+        print(json.dumps({
+            "metric": METRIC, "workload": "kicked Ising, 127-qubit heavy-hex", "value": world * n_steps / elapsed,
+            "unit": "Trotter steps/s", "n_gpus": world, "steps": n_steps, "warmup": 0,
+            "ms_per_step": elapsed / n_steps * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+            "config": {"lattice": "heavy-hex, 127 qubits, 144 edges", "chi": 32, "theta": 0.6,
+                       "gates": "RX(0.6) on all qubits, RZZ(-pi/2) on all edges in 3 colour classes",
+                       "regauge": "after each colour class, BP accuracy 1e-5"},
+            "max_bond": int(em._layout.edge_chi.max()),
+            "z_mean_final": float(np.mean(z[-1])), "z_target_final": float(z[-1][62]),
+            "clocks": clk.summary(),
+        }), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--workload", choices=["bp", "anneal", "grad"], default="bp",
+    ap.add_argument("--workload", choices=["bp", "anneal", "grad", "ising3d", "eagle"], default="bp",
                     help="bp: BP sweep on the 1024-node chi=16 graph (default); anneal: batched annealing; "
-                         "grad: gradient of the final annealing energy w.r.t. the schedule")
+                         "grad: gradient of the final annealing energy w.r.t. the schedule; ising3d: 3-D Ising "
+                         "canonicalisation; eagle: kicked Ising on the 127-qubit heavy-hex lattice")
     ap.add_argument("--grad-nodes", type=int, default=512)
     ap.add_argument("--instances", type=int, default=64)
     ap.add_argument("--chi", type=int, default=8)
@@ -576,6 +661,10 @@ def main():
             run_anneal(args, world, rank, local)
         elif args.workload == "grad":
             run_grad(args, world, rank, local)
+        elif args.workload == "ising3d":
+            run_ising3d(args, world, rank, local)
+        elif args.workload == "eagle":
+            run_eagle(args, world, rank, local)
         else:
             run_ours(args, world, rank, local)
     finally:
