@@ -51,9 +51,15 @@ def ising_sqrt_partition(
     key: int = 42,
     traversal_type: str = "dfs",
     max_iterations: int = 500,
+    graphed: bool = False,
 ) -> CanonicalizationResult:
     """BP + Vidal gauge on the square-root Ising network for each beta
-    (bond dimension 2, physical dimension 2, FP64)."""
+    (bond dimension 2, physical dimension 2, FP64). ``graphed`` replays each
+    iteration (sweep, gauge, distance) as a CUDA graph (BPEngine.canonicalise);
+    the results are the eager loop's. It is off by default: on the 6x6x6
+    lattice an iteration is a chain of ~200 dependent level launches whose
+    device-side latency a graph does not remove, and capturing costs more than
+    replay saves over one scan."""
     lattice = get_nd_lattice(list(lattice_sizes), 2, 2, open_boundary)
     eng = BPEngine(lattice, traversal=traversal_type, schedule="sync" if synchronous_update else "async")
     L = eng.layout
@@ -68,13 +74,7 @@ def ising_sqrt_partition(
         n2e = [msg_init((nd, e)) for nd, e in eng.topo.half_ids()]
         e2n = [msg_init((e, nd)) for nd, e in eng.topo.half_ids()]
         eng.load_messages(n2e, e2n)
-        hist = []
-        vd = np.finfo(np.float64).max
-        while vd > accuracy and len(hist) < max_iterations:
-            eng.sweep()
-            G, lam = eng.vidal_gauge(accuracy)
-            vd = float(eng.vidal_distance(G, lam, accuracy))
-            hist.append(vd)
+        hist, G, lam = eng.canonicalise(accuracy, max_iterations, graphed=graphed)
         rho = eng.densities()
         mag = float((2 * rho[:, 0, 0].real - 1).mean())
         res.vidal_dist_per_iter.append(np.array(hist))

@@ -11,6 +11,7 @@ sides, the same BP schedule and the same seeded messages).
 
 import numpy as np
 import pytest
+import torch
 
 from dequantizer_b200 import workloads as W
 from dequantizer_b200 import graph as G
@@ -56,6 +57,44 @@ def test_ising_sqrt_partition_matches_oracle(field):
         assert res.number_of_iterations[i] == len(hist)
         assert np.abs(res.vidal_dist_per_iter[i] - np.array(hist)).max() < 1e-9
         assert abs(res.average_magnetization[i] - mag) < 1e-9
+
+
+@pytest.mark.parametrize("sync", [False, True])
+def test_graphed_canonicalisation_equals_eager(sync):
+    """BPEngine.canonicalise with graph replays (one graph per buffer
+    assignment) gives the eager loop's distances, lambdas, final messages and
+    densities bit for bit, at two stopping tolerances (different replay counts)."""
+    from dequantizer_b200.engine import BPEngine
+
+    lat = G.get_nd_lattice([4, 4, 3], 2, 2, True)
+    spins = np.array([1.0, -1.0])
+    init = get_potts_initializer(np.exp(0.3 * np.tensordot(spins, spins, axes=0)), np.exp(-0.15 * spins))
+    runs = {}
+    for graphed in (False, True):
+        for tol in (1e-10, 3e-11):  # two stopping points, so the replay counts differ
+            eng = BPEngine(lat, traversal="dfs", schedule="sync" if sync else "async")
+            eng.load_tensors([init(n) for n in eng.topo.nodes])
+            mi = get_message_random_nonnegative_initializer(42)
+            eng.load_messages([mi((nd, e)) for nd, e in eng.topo.half_ids()],
+                              [mi((e, nd)) for nd, e in eng.topo.half_ids()])
+            hist, Gm, lam = eng.canonicalise(tol, 500, graphed=graphed)
+            runs[(graphed, tol)] = (hist, lam.clone(), eng.n2e.clone(), eng.densities().clone())
+    for tol in (1e-10, 3e-11):
+        a, b = runs[(False, tol)], runs[(True, tol)]
+        assert len(a[0]) > 3 and a[0] == b[0]
+        for x, y in zip(a[1:], b[1:]):
+            assert torch.equal(x, y)
+    # the same engine on reloaded inputs replays its cached graphs from the first iteration
+    eng = BPEngine(lat, traversal="dfs", schedule="sync" if sync else "async")
+    for rep in range(2):
+        eng.load_tensors([init(n) for n in eng.topo.nodes])
+        mi = get_message_random_nonnegative_initializer(42)
+        eng.load_messages([mi((nd, e)) for nd, e in eng.topo.half_ids()],
+                          [mi((e, nd)) for nd, e in eng.topo.half_ids()])
+        hist, Gm, lam = eng.canonicalise(1e-10, 500, graphed=True)
+        assert hist == runs[(False, 1e-10)][0]
+        assert torch.equal(lam, runs[(False, 1e-10)][1])
+        assert torch.equal(eng.densities(), runs[(False, 1e-10)][3])
 
 
 def test_kicked_ising_infinite_cell_matches_oracle():
