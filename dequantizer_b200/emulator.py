@@ -107,6 +107,10 @@ class BPQuantumEmulator:
                 ecap[e] = max(c, 2 * ecap[e])
         if np.array_equal(ncap, L.node_capacity) and np.array_equal(ecap, L.edge_capacity):
             return
+        full = self._full_capacities()
+        if full is not None:  # take the final capacities at once: one arena move instead of one per growing gate
+            ncap = np.maximum(ncap, full[0])
+            ecap = np.maximum(ecap, full[1])
         # queued gates must run first: afterwards host and device bond
         # dimensions agree and the sizes below describe the data on the device
         self._flush()
@@ -123,6 +127,21 @@ class BPQuantumEmulator:
             _lib.call("dqz_repack", self._lam.data_ptr(), lam.data_ptr(), L.d_edge_lam_off.data_ptr(),
                       new.d_edge_lam_off.data_ptr(), cnt.data_ptr(), L.n_edges, 8, stream)
         self._layout, self._G, self._lam = new, G, lam
+
+    # Node-tensor arena size (bytes) at every bond = max_chi below which a
+    # growing state gets those capacities at the first growth.
+    FULL_CAPACITY_BYTES = 2 << 30
+
+    def _full_capacities(self):
+        """(node, edge) capacities with every bond at max_chi, or None when
+        that arena would exceed FULL_CAPACITY_BYTES (then capacities double
+        per growing node instead)."""
+        L = self._layout
+        deg = L.degree.astype(np.float64)
+        if 16.0 * float(np.sum(L.phys.astype(np.float64) * float(self.max_chi) ** deg)) > self.FULL_CAPACITY_BYTES:
+            return None
+        node = L.phys.astype(np.int64) * np.power(np.int64(self.max_chi), L.degree.astype(np.int64))
+        return node, np.full(L.n_edges, self.max_chi, dtype=np.int64)
 
     # ------------------------------------------------------------- API
     @property
