@@ -185,6 +185,12 @@ class GraphLayout:
     def gptr(self):
         return ctypes.byref(self.desc)
 
+    @property
+    def handle(self) -> int:
+        """Address of the table descriptor: the ``graph`` argument of the
+        torch.ops.dqz operators (valid while this layout is alive)."""
+        return ctypes.addressof(self.desc)
+
     # --------------------------------------------------------- capacities
     def max_chi(self) -> int:
         return int(self.edge_chi.max(initial=1))
