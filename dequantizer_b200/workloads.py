@@ -31,7 +31,7 @@ from .initializers import get_message_random_nonnegative_initializer, get_potts_
 HADAMARD = np.sqrt(0.5) * np.array([[1, 1], [1, -1]], dtype=np.complex128)
 
 
-# ----------------------------------------------------------------- config 1
+# ------------------------------------------------ 3-D Ising square-root network
 @dataclass
 class CanonicalizationResult:
     vidal_dist_per_iter: List[np.ndarray] = field(default_factory=list)
@@ -84,7 +84,7 @@ def ising_sqrt_partition(
     return res
 
 
-# ----------------------------------------------------------------- config 3
+# ---------------------------------------------- kicked Ising, heavy-hex lattice
 def kicked_ising_gates(theta: float):
     """RZZ(-pi/2) and RX(theta) (ibm_eagle_processor.py:97-118)."""
     rzz = np.diag(np.exp(np.array([1j, -1j, -1j, 1j]) * np.pi / 4)).reshape((2, 2, 2, 2))
@@ -145,7 +145,7 @@ def run_eagle_simulation(
     return out, em
 
 
-# ----------------------------------------------------------------- config 4
+# ----------------------------------------------------------- quantum annealing
 @dataclass
 class EnergyFunction:
     """J_ij on coupled pairs and fields h_i (energy_function.py)."""

@@ -177,10 +177,10 @@ def test_batched_measurement_sampling_equals_independent_runs():
     U = np.random.default_rng(5).uniform(size=(2, 10))
     ba = BatchedAnnealer(energies, max_chi=4, accuracy=1e-10, max_belief_propagation_iterations=200)
     ba.run(steps)
-    configs = ba.sample_measurements(samples=U)
+    spin_configs = ba.sample_measurements(samples=U)
     for k, en in enumerate(energies):
         res = W.run_quantum_annealer(en, steps, key=1, max_chi=4, gates_number_per_regauging=en.edges_number,
                                      accuracy=1e-10, max_belief_propagation_iterations=200,
                                      synchronous_update=True, sample_measurements=True, samples=U[k])
-        assert np.array_equal(configs[k], res.configuration)
-        assert set(np.unique(configs[k])) <= {-1, 1}
+        assert np.array_equal(spin_configs[k], res.configuration)
+        assert set(np.unique(spin_configs[k])) <= {-1, 1}
