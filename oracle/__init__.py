@@ -7,10 +7,17 @@ tensor-valued TensorGraph methods and the emulators). Only ``tests/``,
 and only as the checker or as the timed CPU baseline. The product package
 ``dequantizer_b200`` never imports it and has no CPU fallback.
 
-Pinning: the reference is pure Python on JAX, and JAX cannot be installed in
-this environment, so it cannot be run to produce golden vectors, and the
-reference ships none. The oracle is pinned instead by the reference's own
-known-answer tests, restated in tests/test_oracle_known_answers.py:
+Pinning, two ways.
+Golden vectors of the reference's own code: tests/golden/make_golden.py runs
+the reference's dequantizer/src/tensor_ops.py as it is. JAX is absent, so it
+runs under a stand-in whose jax.numpy forwards to numpy, with JAX's
+immutable-array meaning of in-place operators. It records inputs and outputs
+of pass_through_node, edge_svd, absorb_by_node, vidal_dist, canonicalize,
+_decompose_gate, _apply_half_gate and simple_update
+(tests/golden/tensor_ops_golden.npz), and tests/test_golden_reference.py
+holds every oracle function to them (1e-12, 1e-10 where SVD vectors enter).
+The reference's own known-answer tests, restated in
+tests/test_oracle_known_answers.py:
   * dequantizer/src/mappings/utils_testing.py:20-100 (random-tree GHZ gauge
     fixing: Vidal distance, truncation to d, messages = I/d, rho = I/d);
   * dequantizer/src/graph/tensor_graph.py:1075-1177 (GHZ preparation and
@@ -19,5 +26,5 @@ known-answer tests, restated in tests/test_oracle_known_answers.py:
     emulator vs the dense exact emulator on the heavy cube, small heavy hex and
     a random tree);
   * dequantizer/src/graph/test_unit.py:8-36 (GHZ core, bloated GHZ).
-Bitwise/LAPACK-level parity with JAX and JAX-PRNG stream parity are unpinned.
+Parity with JAX's own LAPACK calls and with the JAX PRNG stream is unpinned.
 """

@@ -1,0 +1,204 @@
+"""Generates tests/golden/tensor_ops_golden.npz: inputs and outputs of the
+reference's own hot-path functions (dequantizer/src/tensor_ops.py of
+LuchnikovI/dequantizer), for pinning the oracle.
+
+JAX is not installed where this runs and cannot be, so the reference module
+is imported under a minimal stand-in package named ``jax``: ``jax.numpy``
+forwards to numpy, ``jax.scipy.special.entr`` is scipy's and ``jax.Array`` is
+a type name only. Every call the module makes (tensordot, transpose,
+linalg.eigh / svd / qr, norm, trace, sqrt, cumsum, finfo, newaxis, entr)
+exists with the same meaning in numpy / scipy. JAX arrays are immutable:
+``x *= y`` rebinds ``x`` to a new array. numpy would write into the array
+instead, and the reference relies on the JAX meaning (``up_part = tensor;
+up_part *= ...`` in vidal_dist must leave ``tensor`` alone), so every array
+the stand-in hands out is an ndarray subclass whose in-place operators
+return new arrays. The module is the reference's source as it is.
+
+Usage: python tests/golden/make_golden.py [path to the reference checkout]
+"""
+
+import importlib.util
+import os
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+JNP_SHIM = """
+import types as _types
+import numpy as _np
+
+
+class JArray(_np.ndarray):
+    # in-place operators rebind, as for immutable JAX arrays
+    def __iadd__(self, o):
+        return _np.add(self, o)
+
+    def __isub__(self, o):
+        return _np.subtract(self, o)
+
+    def __imul__(self, o):
+        return _np.multiply(self, o)
+
+    def __itruediv__(self, o):
+        return _np.true_divide(self, o)
+
+    def __ipow__(self, o):
+        return _np.power(self, o)
+
+
+def wrap(x):
+    if isinstance(x, _np.ndarray) and not isinstance(x, JArray):
+        return x.view(JArray)
+    if isinstance(x, tuple):
+        return tuple(wrap(y) for y in x)
+    if isinstance(x, list):
+        return [wrap(y) for y in x]
+    return x
+
+
+def _wrapped(fn):
+    def call(*a, **k):
+        return wrap(fn(*a, **k))
+    return call
+
+
+class _Module:
+    def __init__(self, mod):
+        self._mod = mod
+
+    def __getattr__(self, name):
+        obj = getattr(self._mod, name)
+        if isinstance(obj, (_types.FunctionType, _types.BuiltinFunctionType, _np.ufunc)):
+            return _wrapped(obj)
+        if isinstance(obj, _types.ModuleType):
+            return _Module(obj)
+        return obj
+
+
+linalg = _Module(_np.linalg)
+newaxis = None
+
+
+def __getattr__(name):
+    return getattr(_Module(_np), name)
+"""
+
+
+def load_reference(ref_root):
+    shim = tempfile.mkdtemp()
+    os.makedirs(os.path.join(shim, "jax", "numpy"))
+    os.makedirs(os.path.join(shim, "jax", "scipy"))
+    with open(os.path.join(shim, "jax", "__init__.py"), "w") as f:
+        f.write("Array = object\n")
+    with open(os.path.join(shim, "jax", "numpy", "__init__.py"), "w") as f:
+        f.write(JNP_SHIM)
+    with open(os.path.join(shim, "jax", "scipy", "__init__.py"), "w") as f:
+        f.write("")
+    with open(os.path.join(shim, "jax", "scipy", "special.py"), "w") as f:
+        f.write("from scipy.special import entr\n")
+    sys.path.insert(0, shim)
+    path = os.path.join(ref_root, "dequantizer", "src", "tensor_ops.py")
+    spec = importlib.util.spec_from_file_location("reference_tensor_ops", path)
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def crandn(rng, *shape):
+    return rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
+
+
+def psd(rng, n, rank=None):
+    a = crandn(rng, n, rank or n)
+    m = a @ a.conj().T
+    return m / np.trace(m).real
+
+
+def unitary(rng, n):
+    q, r = np.linalg.qr(crandn(rng, n, n))
+    return q * (np.diag(r) / np.abs(np.diag(r)))
+
+
+def cp(x):
+    """Inputs for a reference call: copies, as the stand-in's immutable-semantics arrays."""
+    import jax.numpy as jnp_shim
+
+    return jnp_shim.wrap([np.array(y, copy=True) for y in x] if isinstance(x, list) else np.array(x, copy=True))
+
+
+def main(ref_root):
+    R = load_reference(ref_root)
+    rng = np.random.default_rng(20261203)
+    out = {}
+
+    def put(case, name, v):
+        if isinstance(v, (list, tuple)):
+            for i, x in enumerate(v):
+                out[f"{case}/{name}{i}"] = np.array(np.asarray(x))
+            out[f"{case}/{name}_n"] = np.array(len(v))
+        else:
+            out[f"{case}/{name}"] = np.array(np.asarray(v))
+
+    # pass_through_node (tensor_ops.py:36-60)
+    for case, shape in [("ptn_k2", (3, 4, 2)), ("ptn_k3", (2, 3, 4, 2)), ("ptn_k4", (2, 3, 2, 2, 2)),
+                        ("ptn_k3_d3", (2, 2, 3, 3))]:
+        t = crandn(rng, *shape)
+        msgs = [psd(rng, d) for d in shape[:-1]]
+        put(case, "tensor", t)
+        put(case, "msg", msgs)
+        put(case, "out", R.pass_through_node(cp(t), cp(msgs)))
+    # edge_svd (tensor_ops.py:108-130), full rank and rank deficient
+    for case, ranks in [("esvd_full", (None, None)), ("esvd_def", (2, 3))]:
+        ms = [psd(rng, 4, ranks[0]), psd(rng, 4, ranks[1])]
+        orth, lam = R.edge_svd(cp(ms), 1e-10)
+        put(case, "msg", ms)
+        put(case, "orth", orth)
+        put(case, "lam", lam)
+    # absorb_by_node (tensor_ops.py:88-93)
+    t = crandn(rng, 2, 3, 4, 2)
+    mats = [crandn(rng, d, d) for d in (2, 3, 4)]
+    put("abs_k3", "tensor", t)
+    put("abs_k3", "mat", mats)
+    put("abs_k3", "out", R.absorb_by_node(cp(t), cp(mats)))
+    # vidal_dist (tensor_ops.py:143-175) and canonicalize (tensor_ops.py:189-199)
+    t = crandn(rng, 2, 3, 4, 2)
+    lams = [np.array([0.8, 0.6]), np.array([0.9, 0.4, 1e-12]), np.abs(rng.standard_normal(4)) + 0.1]
+    put("vd_k3", "tensor", t)
+    put("vd_k3", "lam", lams)
+    put("vd_k3", "out", R.vidal_dist(cp(t), cp(lams), 1e-10))
+    put("can_k3", "out", R.canonicalize(cp(t), cp(lams), 1e-10))
+    # _decompose_gate (tensor_ops.py:202-218)
+    cnot = np.eye(4, dtype=complex)[[0, 1, 3, 2]].reshape(2, 2, 2, 2)
+    zz = np.diag(np.exp(1j * np.array([0.3, -0.3, -0.3, 0.3]))).reshape(2, 2, 2, 2)
+    rnd = unitary(rng, 4).reshape(2, 2, 2, 2)
+    for case, gate in [("dg_cnot", cnot), ("dg_zz", zz), ("dg_rand", rnd)]:
+        h1, h2 = R._decompose_gate(cp(gate), 1e-10)
+        put(case, "gate", gate)
+        put(case, "half", [h1, h2])
+    h1, h2 = R._decompose_gate(cp(rnd), 1e-10)
+    # _apply_half_gate (tensor_ops.py:221-237)
+    t = crandn(rng, 2, 3, 2)
+    put("ahg", "tensor", t)
+    put("ahg", "out", R._apply_half_gate(cp(t), cp(h1), 1))
+    # simple_update (tensor_ops.py:318-389): bond 4 between t1's bond 2 and t2's bond 0
+    t1, t2 = crandn(rng, 2, 3, 4, 2), crandn(rng, 4, 3, 2)
+    shared = np.sort(np.abs(rng.standard_normal(4)))[::-1] + 0.05
+    lam1 = [np.abs(rng.standard_normal(2)) + 0.1, np.abs(rng.standard_normal(3)) + 0.1, shared]
+    lam2 = [shared, np.abs(rng.standard_normal(3)) + 0.1]
+    for case, acc, rank in [("su_acc", 1e-2, None), ("su_rank", None, 3)]:
+        res = R.simple_update(cp(t1), cp(t2), cp(lam1), cp(lam2), cp(h1), cp(h2), 2, 0, 1e-10, acc, rank)
+        put(case, "t", [t1, t2])
+        put(case, "lam1", lam1)
+        put(case, "lam2", lam2)
+        put(case, "half", [h1, h2])
+        put(case, "out", [res[0], res[1], res[2], np.array(res[3]), np.array(res[4])])
+    np.savez_compressed(os.path.join(HERE, "tensor_ops_golden.npz"), **out)
+    print(f"{len(out)} arrays written")
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
