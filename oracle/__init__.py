@@ -16,6 +16,10 @@ of pass_through_node, edge_svd, absorb_by_node, vidal_dist, canonicalize,
 _decompose_gate, _apply_half_gate and simple_update
 (tests/golden/tensor_ops_golden.npz), and tests/test_golden_reference.py
 holds every oracle function to them (1e-12, 1e-10 where SVD vectors enter).
+The same script runs the reference's maps (BP in its four schedules, Vidal
+gauge and distance, symmetric gauge, lambdas2messages, message distance,
+density matrices) on three deterministic graphs (tests/golden/maps_golden.npz);
+tests/test_golden_maps.py holds the oracle's maps and traversals to them.
 The reference's own known-answer tests, restated in
 tests/test_oracle_known_answers.py:
   * dequantizer/src/mappings/utils_testing.py:20-100 (random-tree GHZ gauge

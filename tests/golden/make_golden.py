@@ -1,6 +1,7 @@
-"""Generates tests/golden/tensor_ops_golden.npz: inputs and outputs of the
-reference's own hot-path functions (dequantizer/src/tensor_ops.py of
-LuchnikovI/dequantizer), for pinning the oracle.
+"""Generates tests/golden/tensor_ops_golden.npz and tests/golden/maps_golden.npz:
+inputs and outputs of the reference's own hot-path functions
+(dequantizer/src/tensor_ops.py of LuchnikovI/dequantizer) and of its maps
+(dequantizer/src/mappings) on deterministic graphs, for pinning the oracle.
 
 JAX is not installed where this runs and cannot be, so the reference module
 is imported under a minimal stand-in package named ``jax``: ``jax.numpy``
@@ -72,10 +73,10 @@ class _Module:
 
     def __getattr__(self, name):
         obj = getattr(self._mod, name)
-        if isinstance(obj, (_types.FunctionType, _types.BuiltinFunctionType, _np.ufunc)):
-            return _wrapped(obj)
         if isinstance(obj, _types.ModuleType):
             return _Module(obj)
+        if callable(obj) and not isinstance(obj, type):  # functions, ufuncs, array-function dispatchers
+            return _wrapped(obj)
         return obj
 
 
@@ -88,12 +89,49 @@ def __getattr__(name):
 """
 
 
+# The package imports jit (maps are plain functions here), jax.config, the
+# PRNG (never called: every input below is given explicitly) and
+# lax.dynamic_slice (TensorGraph.truncate).
+JAX_SHIM = """
+Array = object
+
+
+def jit(f, *args, **kwargs):
+    return f
+
+
+class _Config:
+    def update(self, *args, **kwargs):
+        pass
+
+
+config = _Config()
+"""
+
+RANDOM_SHIM = """
+def _unavailable(*args, **kwargs):
+    raise RuntimeError("the JAX PRNG is not available under the stand-in")
+
+
+PRNGKey = split = randint = normal = uniform = _unavailable
+"""
+
+LAX_SHIM = """
+def dynamic_slice(operand, start_indices, slice_sizes):
+    return operand[tuple(slice(int(s), int(s) + int(n)) for s, n in zip(start_indices, slice_sizes))]
+"""
+
+
 def load_reference(ref_root):
     shim = tempfile.mkdtemp()
     os.makedirs(os.path.join(shim, "jax", "numpy"))
     os.makedirs(os.path.join(shim, "jax", "scipy"))
     with open(os.path.join(shim, "jax", "__init__.py"), "w") as f:
-        f.write("Array = object\n")
+        f.write(JAX_SHIM)
+    with open(os.path.join(shim, "jax", "random.py"), "w") as f:
+        f.write(RANDOM_SHIM)
+    with open(os.path.join(shim, "jax", "lax.py"), "w") as f:
+        f.write(LAX_SHIM)
     with open(os.path.join(shim, "jax", "numpy", "__init__.py"), "w") as f:
         f.write(JNP_SHIM)
     with open(os.path.join(shim, "jax", "scipy", "__init__.py"), "w") as f:
@@ -134,6 +172,8 @@ def main(ref_root):
     R = load_reference(ref_root)
     rng = np.random.default_rng(20261203)
     out = {}
+
+    import jax.numpy as jnp_shim
 
     def put(case, name, v):
         if isinstance(v, (list, tuple)):
@@ -198,6 +238,83 @@ def main(ref_root):
         put(case, "out", [res[0], res[1], res[2], np.array(res[3]), np.array(res[4])])
     np.savez_compressed(os.path.join(HERE, "tensor_ops_golden.npz"), **out)
     print(f"{len(out)} arrays written")
+    maps_golden(ref_root)
+
+
+MAP_GRAPHS = {  # name -> (constructor name, arguments): the same constructors exist in dequantizer_b200.graph
+    "lat232": ("get_nd_lattice", ([2, 3, 2], 2, 2, True)),
+    "lat222_chi3": ("get_nd_lattice", ([2, 2, 2], 2, 3, True)),
+    "hexinf": ("get_heavy_hex_ibm_eagle_lattice_infinite", ()),
+}
+
+
+def maps_golden(ref_root):
+    """Inputs and outputs of the reference's maps (dequantizer/src/mappings)
+    on deterministic graphs, keyed by graph, quantity and repr of the element
+    or message ID."""
+    sys.path.insert(0, ref_root)
+    import jax.numpy as jnp_shim
+
+    import dequantizer as D
+
+    rng = np.random.default_rng(7)
+    out = {}
+    for gname, (ctor, args) in MAP_GRAPHS.items():
+        graph = getattr(D, ctor)(*args)
+        for ordering in ("dfs", "bfs"):
+            trav = list(graph.get_traversal_iterator(ordering=ordering))
+            out[f"{gname}/traversal_{ordering}"] = np.array([repr(el.id) for el in trav])
+        trav = list(graph.get_traversal_iterator())
+
+        def tensor_init(node):
+            return jnp_shim.wrap(crandn(rng, *node.bond_shape, node.dimension))
+
+        def message_init(md):
+            d = md[0].dimension if isinstance(md[0], D.Edge) else md[1].dimension
+            return jnp_shim.wrap(psd(rng, d))
+
+        tensors = graph.init_tensors(tensor_init)
+        messages = graph.init_messages(message_init)
+
+        def put(what, d):
+            """One dict as three arrays: repr keys, the shapes, the flat values.
+            Every array the reference returned must carry the stand-in's
+            immutable semantics (a plain ndarray would mean an in-place operator
+            could have written into an input)."""
+            assert all(isinstance(v, jnp_shim.JArray) for v in d.values()), what
+            arrs = [np.array(np.asarray(v)) for v in d.values()]
+            out[f"{gname}/{what}/keys"] = np.array([repr(k) for k in d])
+            out[f"{gname}/{what}/ndim"] = np.array([a.ndim for a in arrs])
+            out[f"{gname}/{what}/dims"] = np.array([n for a in arrs for n in a.shape], dtype=np.int64)
+            out[f"{gname}/{what}/data"] = np.concatenate([a.ravel().astype(np.complex128) for a in arrs])
+
+        put("tensors", tensors)
+        put("messages", messages)
+        for ordering in ("dfs", "bfs"):
+            t_ord = list(graph.get_traversal_iterator(ordering=ordering))
+            for sync in (False, True):
+                bp = D.get_belief_propagation_map(t_ord, sync)
+                m = messages
+                for _ in range(2):
+                    m = bp(tensors, m)
+                put(f"bp2_{ordering}_{'sync' if sync else 'async'}", m)
+        bp = D.get_belief_propagation_map(trav)
+        m = messages
+        for _ in range(30):
+            m = bp(tensors, m)
+        put("messages_30", m)
+        m_next = bp(tensors, m)
+        out[f"{gname}/frob_30_31"] = np.array(float(D.messages_frob_distance(m, m_next)))
+        g_t, lam = D.get_vidal_gauge_fixing_map(trav, 1e-10)(tensors, m)
+        put("vidal_tensors", g_t)
+        put("vidal_lambdas", lam)
+        out[f"{gname}/vidal_distance"] = np.array(float(D.get_vidal_gauge_distance_map(trav, 1e-10)(g_t, lam)))
+        put("symmetric_tensors", D.get_symmetric_gauge_fixing_map(trav, 1e-10)(g_t, lam))
+        put("lambda_messages", D.lambdas2messages(lam))
+        rho = {el.id: D.get_one_side_density_matrix(el, tensors, m) for el in trav if isinstance(el, D.Node)}
+        put("density", rho)
+    np.savez_compressed(os.path.join(HERE, "maps_golden.npz"), **out)
+    print(f"{len(out)} map arrays written")
 
 
 if __name__ == "__main__":

@@ -1,0 +1,121 @@
+"""The oracle's maps against the reference's own maps on deterministic graphs.
+
+tests/golden/maps_golden.npz (tests/golden/make_golden.py) holds, for a
+2x3x2 lattice (bond 2), a 2x2x2 lattice (bond 3) and the infinite heavy-hex
+cell, what the reference's dequantizer/src/mappings produce:
+* the DFS and BFS traversal orders;
+* two BP sweeps in each schedule (asynchronous / synchronous, DFS / BFS order)
+  from seeded tensors and messages;
+* after 30 asynchronous sweeps: the message distance to the next sweep, the
+  Vidal gauge (tensors and lambdas), the Vidal distance, the symmetric gauge,
+  lambdas2messages and every node's one-site density matrix.
+Graphs come from this package's own constructors, so the traversal check
+also pins the graph structure. Each oracle map gets the reference's inputs
+and must give its outputs (1e-12; 1e-10 after 30 sweeps and where
+eigen / singular vectors enter).
+"""
+
+import os
+
+import numpy as np
+import pytest
+
+from dequantizer_b200 import graph as G
+from dequantizer_b200.graph import Node
+from oracle import maps as OM
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "maps_golden.npz")
+GRAPHS = {
+    "lat232": lambda: G.get_nd_lattice([2, 3, 2], 2, 2, True),
+    "lat222_chi3": lambda: G.get_nd_lattice([2, 2, 2], 2, 3, True),
+    "hexinf": G.get_heavy_hex_ibm_eagle_lattice_infinite,
+}
+
+
+@pytest.fixture(scope="module")
+def gold():
+    return dict(np.load(GOLDEN))
+
+
+def unpack(gold, prefix):
+    """repr(key) -> array of one recorded dict."""
+    keys = gold[f"{prefix}/keys"]
+    ndim, dims, data = gold[f"{prefix}/ndim"], gold[f"{prefix}/dims"], gold[f"{prefix}/data"]
+    out, d0, v0 = {}, 0, 0
+    for k, nd in zip(keys, ndim):
+        shape = tuple(int(x) for x in dims[d0:d0 + nd])
+        n = int(np.prod(shape)) if shape else 1
+        out[str(k)] = data[v0:v0 + n].reshape(shape)
+        d0, v0 = d0 + nd, v0 + n
+    return out
+
+
+def keyed(graph, recorded, real=False):
+    """A recorded dict re-keyed by this package's IDs (elements and messages)."""
+    ids = {}
+    for el in graph.get_traversal_iterator():
+        ids[repr(el.id)] = el.id
+    for k in graph.init_messages(lambda md: None):
+        ids[repr(k)] = k
+    return {ids[k]: (v.real if real else v) for k, v in recorded.items()}
+
+
+def close(a, b, tol):
+    a, b = np.asarray(a), np.asarray(b)
+    assert a.shape == b.shape
+    assert np.abs(a - b).max() <= tol * max(np.abs(b).max(), 1e-300)
+
+
+def close_dicts(a, recorded, tol):
+    """``a`` keyed by IDs, ``recorded`` by their repr."""
+    assert set(map(repr, a)) == set(recorded)
+    for k, v in a.items():
+        close(v, recorded[repr(k)], tol)
+
+
+@pytest.mark.parametrize("name", list(GRAPHS))
+def test_traversals_match(gold, name):
+    graph = GRAPHS[name]()
+    for ordering in ("dfs", "bfs"):
+        ours = [repr(el.id) for el in graph.get_traversal_iterator(ordering=ordering)]
+        assert ours == [str(x) for x in gold[f"{name}/traversal_{ordering}"]]
+    assert [repr(el.id) for el in graph.get_traversal_iterator()] == [str(x) for x in gold[f"{name}/traversal_bfs"]]
+
+
+@pytest.mark.parametrize("name", list(GRAPHS))
+@pytest.mark.parametrize("ordering", ["dfs", "bfs"])
+@pytest.mark.parametrize("sync", [False, True])
+def test_bp_sweeps_match(gold, name, ordering, sync):
+    graph = GRAPHS[name]()
+    tensors = keyed(graph, unpack(gold, f"{name}/tensors"))
+    m = keyed(graph, unpack(gold, f"{name}/messages"))
+    bp = OM.get_belief_propagation_map(list(graph.get_traversal_iterator(ordering=ordering)), sync)
+    for _ in range(2):
+        m = bp(tensors, m)
+    close_dicts(m, unpack(gold, f"{name}/bp2_{ordering}_{'sync' if sync else 'async'}"), 1e-12)
+
+
+@pytest.mark.parametrize("name", list(GRAPHS))
+def test_gauges_distances_and_densities_match(gold, name):
+    graph = GRAPHS[name]()
+    trav = list(graph.get_traversal_iterator())
+    tensors = keyed(graph, unpack(gold, f"{name}/tensors"))
+    m0 = keyed(graph, unpack(gold, f"{name}/messages"))
+    bp = OM.get_belief_propagation_map(trav)
+    m = m0
+    for _ in range(30):
+        m = bp(tensors, m)
+    close_dicts(m, unpack(gold, f"{name}/messages_30"), 1e-10)
+    m30 = keyed(graph, unpack(gold, f"{name}/messages_30"))
+    close(OM.messages_frob_distance(m30, bp(tensors, m30)), gold[f"{name}/frob_30_31"], 1e-10)
+    g_t, lam = OM.get_vidal_gauge_fixing_map(trav, 1e-10)(tensors, m30)
+    close_dicts(g_t, unpack(gold, f"{name}/vidal_tensors"), 1e-10)
+    close_dicts(lam, {k: v.real for k, v in unpack(gold, f"{name}/vidal_lambdas").items()}, 1e-10)
+    gv_t = keyed(graph, unpack(gold, f"{name}/vidal_tensors"))
+    gv_l = keyed(graph, unpack(gold, f"{name}/vidal_lambdas"), real=True)
+    close(OM.get_vidal_gauge_distance_map(trav, 1e-10)(gv_t, gv_l), gold[f"{name}/vidal_distance"], 1e-10)
+    close_dicts(OM.get_symmetric_gauge_fixing_map(trav, 1e-10)(gv_t, gv_l),
+                unpack(gold, f"{name}/symmetric_tensors"), 1e-12)
+    close_dicts(OM.lambdas2messages(gv_l), unpack(gold, f"{name}/lambda_messages"), 1e-12)
+    rho = {el.id: OM.get_one_side_density_matrix(el, tensors, m30) for el in trav if isinstance(el, Node)}
+    close_dicts(rho, unpack(gold, f"{name}/density"), 1e-12)
