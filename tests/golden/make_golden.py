@@ -313,8 +313,45 @@ def maps_golden(ref_root):
         put("lambda_messages", D.lambdas2messages(lam))
         rho = {el.id: D.get_one_side_density_matrix(el, tensors, m) for el in trav if isinstance(el, D.Node)}
         put("density", rho)
+        if gname == "lat232":
+            graph_ops(D, graph, out, put, g_t, lam, rng)
     np.savez_compressed(os.path.join(HERE, "maps_golden.npz"), **out)
     print(f"{len(out)} map arrays written")
+
+
+def graph_ops(D, graph, out, put, tensors, lambdas, rng):
+    """TensorGraph.apply1 / apply2_to_vidal_canonical / truncate / apply2
+    (tensor_graph.py:235-446) from the lattice's Vidal form; the gate
+    methods also change the graph's bond dimensions, recorded after each step."""
+    import jax.numpy as jnp_shim
+
+    edges = [el for el in graph.get_traversal_iterator(ordering="dfs") if isinstance(el, D.Edge)]
+    rx = jnp_shim.wrap(np.array([[np.cos(0.3), -1j * np.sin(0.3)], [-1j * np.sin(0.3), np.cos(0.3)]]))
+    cnot = jnp_shim.wrap(np.eye(4, dtype=complex)[[0, 1, 3, 2]].reshape(2, 2, 2, 2))
+    zz = jnp_shim.wrap(np.diag(np.exp(1j * np.array([0.3, -0.3, -0.3, 0.3]))).reshape(2, 2, 2, 2))
+    rnd = jnp_shim.wrap(unitary(rng, 4).reshape(2, 2, 2, 2))
+    out["ops/gate_rnd"] = np.array(np.asarray(rnd))
+    tensors, lambdas = dict(tensors), dict(lambdas)
+    first = next(el for el in graph.get_traversal_iterator(ordering="dfs") if isinstance(el, D.Node))
+    tensors = graph.apply1(first.id, tensors, rx)
+    put("ops/after_apply1", tensors)
+    steps = [(cnot, edges[0], None, 3), (rnd, edges[1], 1e-3, None), (zz, edges[2], None, None)]
+    for i, (gate, edge, acc, rank) in enumerate(steps):
+        a, b = edge.id
+        tensors, lambdas, err, ent = graph.apply2_to_vidal_canonical(a, b, tensors, lambdas, gate, 1e-10, acc, rank)
+        put(f"ops/step{i}_tensors", tensors)
+        put(f"ops/step{i}_lambdas", lambdas)
+        out[f"ops/step{i}_err"] = np.array(float(err))
+        out[f"ops/step{i}_entropy"] = np.array(float(ent))
+        out[f"ops/step{i}_edge_dims"] = np.array([e.dimension for e in edges])
+    tensors, lambdas = graph.truncate(tensors, lambdas, 1e-2)
+    put("ops/truncated_tensors", tensors)
+    put("ops/truncated_lambdas", lambdas)
+    out["ops/truncated_edge_dims"] = np.array([e.dimension for e in edges])
+    a, b = edges[3].id
+    tensors = graph.apply2(a, b, tensors, rnd, 1e-10)
+    put("ops/apply2_tensors", tensors)
+    out["ops/apply2_edge_dims"] = np.array([e.dimension for e in edges])
 
 
 if __name__ == "__main__":

@@ -119,3 +119,41 @@ def test_gauges_distances_and_densities_match(gold, name):
     close_dicts(OM.lambdas2messages(gv_l), unpack(gold, f"{name}/lambda_messages"), 1e-12)
     rho = {el.id: OM.get_one_side_density_matrix(el, tensors, m30) for el in trav if isinstance(el, Node)}
     close_dicts(rho, unpack(gold, f"{name}/density"), 1e-12)
+
+
+def test_graph_gate_methods_match(gold):
+    """TensorGraph.apply1 / apply2_to_vidal_canonical (rank cap, accuracy
+    cap, none) / truncate / apply2 from the 2x3x2 lattice's Vidal form, as
+    the reference ran them: tensors, lambdas, truncation errors, entropies
+    and the bond dimensions the methods leave on the graph."""
+    from dequantizer_b200.graph import Edge
+
+    graph = GRAPHS["lat232"]()
+    edges = [el for el in graph.get_traversal_iterator(ordering="dfs") if isinstance(el, Edge)]
+    tensors = keyed(graph, unpack(gold, "lat232/vidal_tensors"))
+    lambdas = keyed(graph, unpack(gold, "lat232/vidal_lambdas"), real=True)
+    rx = np.array([[np.cos(0.3), -1j * np.sin(0.3)], [-1j * np.sin(0.3), np.cos(0.3)]])
+    cnot = np.eye(4, dtype=complex)[[0, 1, 3, 2]].reshape(2, 2, 2, 2)
+    zz = np.diag(np.exp(1j * np.array([0.3, -0.3, -0.3, 0.3]))).reshape(2, 2, 2, 2)
+    rnd = gold["ops/gate_rnd"]
+    first = next(el for el in graph.get_traversal_iterator(ordering="dfs") if isinstance(el, Node))
+    tensors = OM.apply1(graph, first.id, tensors, rx)
+    close_dicts(tensors, unpack(gold, "lat232/ops/after_apply1"), 1e-12)
+    steps = [(cnot, edges[0], None, 3), (rnd, edges[1], 1e-3, None), (zz, edges[2], None, None)]
+    for i, (gate, edge, acc, rank) in enumerate(steps):
+        a, b = edge.id
+        tensors, lambdas, err, ent = OM.apply2_to_vidal_canonical(graph, a, b, tensors, lambdas, gate, 1e-10, acc,
+                                                                  rank)
+        close_dicts(tensors, unpack(gold, f"lat232/ops/step{i}_tensors"), 1e-10)
+        close_dicts(lambdas, {k: v.real for k, v in unpack(gold, f"lat232/ops/step{i}_lambdas").items()}, 1e-10)
+        close(err, gold[f"ops/step{i}_err"], 1e-8)
+        close(ent, gold[f"ops/step{i}_entropy"], 1e-10)
+        assert [e.dimension for e in edges] == list(gold[f"ops/step{i}_edge_dims"])
+    tensors, lambdas = OM.truncate(graph, tensors, lambdas, 1e-2)
+    close_dicts(tensors, unpack(gold, "lat232/ops/truncated_tensors"), 1e-10)
+    close_dicts(lambdas, {k: v.real for k, v in unpack(gold, "lat232/ops/truncated_lambdas").items()}, 1e-10)
+    assert [e.dimension for e in edges] == list(gold["ops/truncated_edge_dims"])
+    a, b = edges[3].id
+    tensors = OM.apply2(graph, a, b, tensors, rnd, 1e-10)
+    close_dicts(tensors, unpack(gold, "lat232/ops/apply2_tensors"), 1e-10)
+    assert [e.dimension for e in edges] == list(gold["ops/apply2_edge_dims"])
