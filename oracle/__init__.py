@@ -19,7 +19,10 @@ holds every oracle function to them (1e-12, 1e-10 where SVD vectors enter).
 The same script runs the reference's maps (BP in its four schedules, Vidal
 gauge and distance, symmetric gauge, lambdas2messages, message distance,
 density matrices) on three deterministic graphs (tests/golden/maps_golden.npz);
-tests/test_golden_maps.py holds the oracle's maps and traversals to them.
+It also records the TensorGraph gate methods on a lattice and a run of the
+reference's BPQuantumEmulator (initial messages drawn as this package's
+emulator draws them). tests/test_golden_maps.py holds the oracle's maps,
+traversals, methods and emulator to these records.
 The reference's own known-answer tests, restated in
 tests/test_oracle_known_answers.py:
   * dequantizer/src/mappings/utils_testing.py:20-100 (random-tree GHZ gauge

@@ -13,7 +13,8 @@ exists with the same meaning in numpy / scipy. JAX arrays are immutable:
 instead, and the reference relies on the JAX meaning (``up_part = tensor;
 up_part *= ...`` in vidal_dist must leave ``tensor`` alone), so every array
 the stand-in hands out is an ndarray subclass whose in-place operators
-return new arrays. The module is the reference's source as it is.
+return new arrays (and whose ``x.at[i].set(v)`` returns an updated copy, as
+in JAX). The module is the reference's source as it is.
 
 Usage: python tests/golden/make_golden.py [path to the reference checkout]
 """
@@ -50,6 +51,29 @@ class JArray(_np.ndarray):
     def __ipow__(self, o):
         return _np.power(self, o)
 
+    @property
+    def at(self):
+        # x.at[idx].set(v): a copy of x with x[idx] = v (JAX's functional update)
+        return _At(self)
+
+
+class _At:
+    def __init__(self, arr):
+        self._arr = arr
+
+    def __getitem__(self, idx):
+        return _AtIndex(self._arr, idx)
+
+
+class _AtIndex:
+    def __init__(self, arr, idx):
+        self._arr, self._idx = arr, idx
+
+    def set(self, value):
+        new = _np.array(self._arr, copy=True).view(JArray)
+        new[self._idx] = value
+        return new
+
 
 def wrap(x):
     if isinstance(x, _np.ndarray) and not isinstance(x, JArray):
@@ -82,6 +106,8 @@ class _Module:
 
 linalg = _Module(_np.linalg)
 newaxis = None
+complex_ = _np.complex128  # JAX's aliases under 64-bit mode
+float_ = _np.float64
 
 
 def __getattr__(name):
@@ -108,12 +134,43 @@ class _Config:
 config = _Config()
 """
 
+# The PRNG stand-in reproduces the draws of this package's oracle emulator:
+# a key holds numpy's default_rng(seed); split() returns the key and its next
+# 31-bit integer (one per Vidal canonicalisation); normal(subkey, shape) is
+# default_rng(subkey).standard_normal(shape). The JAX PRNG stream itself is
+# not reproduced (nothing here depends on it but the choice of start).
 RANDOM_SHIM = """
+import numpy as _np
+
+
+class _Key:
+    def __init__(self, seed):
+        self.rng = _np.random.default_rng(int(seed))
+
+
+def PRNGKey(seed):
+    return _Key(seed)
+
+
+def split(key, num=2):
+    if not isinstance(key, _Key) or num != 2:
+        raise RuntimeError("split(key) of a PRNGKey only")
+    return key, int(key.rng.integers(0, 2**31 - 1))
+
+
+def normal(key, shape):
+    from jax.numpy import wrap
+
+    if isinstance(key, _Key):
+        raise RuntimeError("normal() of a split subkey only")
+    return wrap(_np.random.default_rng(int(key)).standard_normal(shape))
+
+
 def _unavailable(*args, **kwargs):
-    raise RuntimeError("the JAX PRNG is not available under the stand-in")
+    raise RuntimeError("not available under the stand-in")
 
 
-PRNGKey = split = randint = normal = uniform = _unavailable
+randint = uniform = _unavailable
 """
 
 LAX_SHIM = """
@@ -315,8 +372,39 @@ def maps_golden(ref_root):
         put("density", rho)
         if gname == "lat232":
             graph_ops(D, graph, out, put, g_t, lam, rng)
+    emulator(D, out)
     np.savez_compressed(os.path.join(HERE, "maps_golden.npz"), **out)
     print(f"{len(out)} map arrays written")
+
+
+def emulator(D, out):
+    """BPQuantumEmulator (bp_quantum_emulator.py:50-300) on the infinite
+    heavy-hex cell: key 42, bond dimension <= 4, regauge after every layer of
+    two-site gates (BP accuracy 1e-7, at most 100 iterations), three layers
+    of RX(0.8) on every qubit and RZZ(-pi/2) on every edge in traversal order.
+    Recorded: every qubit's density matrix after each layer, and the
+    emulator's truncation errors, entropies and Vidal distances."""
+    import jax.numpy as jnp_shim
+    from jax.random import PRNGKey
+
+    lat = D.get_heavy_hex_ibm_eagle_lattice_infinite()
+    trav = list(lat.get_traversal_iterator())
+    em = D.BPQuantumEmulator(lat, PRNGKey(42), 4, lat.edges_number, 1e-7, 100)
+    rzz = jnp_shim.wrap(np.diag(np.exp(np.array([1j, -1j, -1j, 1j]) * np.pi / 4)).reshape(2, 2, 2, 2))
+    rx = jnp_shim.wrap(np.array([[np.cos(0.4), -1j * np.sin(0.4)], [-1j * np.sin(0.4), np.cos(0.4)]]))
+    nodes = [el.id for el in trav if isinstance(el, D.Node)]
+    out["emu/nodes"] = np.array([repr(n) for n in nodes])
+    for layer in range(3):
+        for n in nodes:
+            em.apply_q1(rx, n)
+        for el in trav:
+            if isinstance(el, D.Edge):
+                em.apply_q2(rzz, *el.id)
+        out[f"emu/rho_{layer}"] = np.stack([np.asarray(em.dens_q1(n)) for n in nodes])
+    out["emu/truncation_errors"] = np.array([float(x) for x in em.truncation_errors])
+    out["emu/entropies"] = np.array([float(x) for x in em.entropies])
+    out["emu/after_regauging"] = np.array([float(x) for x in np.asarray(em.after_regauging_vidal_distances)])
+    out["emu/truncated_affected"] = np.array([float(x) for x in np.asarray(em.truncated_affected_vidal_distances)])
 
 
 def graph_ops(D, graph, out, put, tensors, lambdas, rng):

@@ -157,3 +157,33 @@ def test_graph_gate_methods_match(gold):
     tensors = OM.apply2(graph, a, b, tensors, rnd, 1e-10)
     close_dicts(tensors, unpack(gold, "lat232/ops/apply2_tensors"), 1e-10)
     assert [e.dimension for e in edges] == list(gold["ops/apply2_edge_dims"])
+
+
+def test_emulator_matches(gold):
+    """The oracle's BPQuantumEmulator against the reference's on the infinite
+    heavy-hex cell (key 42, bond <= 4, regauge per layer, three kicked-Ising
+    layers; the reference's initial messages drawn as the oracle draws them):
+    every qubit's density matrix after each layer, truncation errors,
+    entropies and Vidal distances."""
+    from dequantizer_b200.graph import Edge
+    from oracle.emulator import BPQuantumEmulator as OracleEmulator
+
+    lat = G.get_heavy_hex_ibm_eagle_lattice_infinite()
+    trav = list(lat.get_traversal_iterator())
+    em = OracleEmulator(lat, 42, 4, lat.edges_number, 1e-7, 100)
+    rzz = np.diag(np.exp(np.array([1j, -1j, -1j, 1j]) * np.pi / 4)).reshape(2, 2, 2, 2)
+    rx = np.array([[np.cos(0.4), -1j * np.sin(0.4)], [-1j * np.sin(0.4), np.cos(0.4)]])
+    nodes = [el.id for el in trav if isinstance(el, Node)]
+    assert [repr(n) for n in nodes] == [str(x) for x in gold["emu/nodes"]]
+    for layer in range(3):
+        for n in nodes:
+            em.apply_q1(rx, n)
+        for el in trav:
+            if isinstance(el, Edge):
+                em.apply_q2(rzz, *el.id)
+        close(np.stack([em.dens_q1(n) for n in nodes]), gold[f"emu/rho_{layer}"], 1e-10)
+    assert len(em.truncation_errors) == len(gold["emu/truncation_errors"])
+    assert np.abs(np.array(em.truncation_errors) - gold["emu/truncation_errors"]).max() < 1e-10
+    assert np.abs(np.array(em.entropies) - gold["emu/entropies"]).max() < 1e-10
+    assert np.abs(np.array(em.after_regauging_vidal_distances) - gold["emu/after_regauging"]).max() < 1e-10
+    assert np.abs(np.array(em.truncated_affected_vidal_distances) - gold["emu/truncated_affected"]).max() < 1e-10
