@@ -373,8 +373,44 @@ def maps_golden(ref_root):
         if gname == "lat232":
             graph_ops(D, graph, out, put, g_t, lam, rng)
     emulator(D, out)
+    annealer(ref_root, out)
     np.savez_compressed(os.path.join(HERE, "maps_golden.npz"), **out)
     print(f"{len(out)} map arrays written")
+
+
+def annealer(ref_root, out):
+    """run_quantum_annealer of the reference's annealing example
+    (examples/quantum_annealing/quantum_annealing/src/quantum_annealer.py:90-152,
+    first-order Trotter steps from get_scheduler, scheduler.py:7-14) on a
+    10-spin random 3-regular instance with J = +-1 and random fields: key 7,
+    bond <= 4, a regauge per layer of couplings, BP accuracy 1e-7, six steps of
+    size 0.2 with f(t) = 1 - t. Recorded: the instance, every step's density
+    matrices, truncation errors, entropies and Vidal distances."""
+    from jax.random import PRNGKey
+
+    sys.path.insert(0, os.path.join(ref_root, "examples", "quantum_annealing"))
+    from quantum_annealing.src.energy_function import EnergyFunction
+    from quantum_annealing.src.quantum_annealer import run_quantum_annealer
+    from quantum_annealing.src.scheduler import get_scheduler
+
+    rng = np.random.default_rng(11)
+    n = 10
+    while True:  # pairing-model 3-regular graph without loops or repeated edges
+        stubs = rng.permutation(np.repeat(np.arange(n), 3))
+        pairs = np.sort(stubs.reshape(-1, 2), axis=1)
+        if np.all(pairs[:, 0] != pairs[:, 1]) and len({tuple(p) for p in pairs}) == len(pairs):
+            break
+    amps = rng.choice([-1.0, 1.0], size=len(pairs))
+    fields = 0.5 * rng.standard_normal(n)
+    out["anneal/pairs"], out["anneal/amps"], out["anneal/fields"] = pairs, amps, fields
+    energy = EnergyFunction(amps, pairs, fields)
+    res = run_quantum_annealer(energy, get_scheduler(0.2, lambda t: 1 - t, 6), PRNGKey(7), 4, len(pairs), 1e-7,
+                               100, False, "dfs", False, True)
+    out["anneal/rho_history"] = np.stack([np.asarray(r) for r in res.density_matrices_history])
+    out["anneal/rho"] = np.asarray(res.density_matrices)
+    out["anneal/truncation_errors"] = np.asarray(res.truncation_errors, dtype=float)
+    out["anneal/entropies"] = np.asarray(res.entropies, dtype=float)
+    out["anneal/after_regauging"] = np.array([float(x) for x in np.asarray(res.vidal_distances_after_regauging)])
 
 
 def emulator(D, out):

@@ -187,3 +187,35 @@ def test_emulator_matches(gold):
     assert np.abs(np.array(em.entropies) - gold["emu/entropies"]).max() < 1e-10
     assert np.abs(np.array(em.after_regauging_vidal_distances) - gold["emu/after_regauging"]).max() < 1e-10
     assert np.abs(np.array(em.truncated_affected_vidal_distances) - gold["emu/truncated_affected"]).max() < 1e-10
+
+
+def test_annealer_matches(gold):
+    """The reference's run_quantum_annealer (first-order steps, get_scheduler)
+    against the same loop built from this package's graph, gate and schedule
+    functions (workloads.tensor_graph_of, q1_gate, q2_gate, scheduler,
+    HADAMARD) on the oracle emulator: the density matrices after every step,
+    truncation errors, entropies and Vidal distances after regauging. This
+    pins the annealing gate forms and sign conventions."""
+    from dequantizer_b200 import workloads as W
+    from oracle.emulator import BPQuantumEmulator as OracleEmulator
+
+    energy = W.EnergyFunction(gold["anneal/amps"], gold["anneal/pairs"], gold["anneal/fields"])
+    g = W.tensor_graph_of(energy)
+    em = OracleEmulator(g, 7, 4, len(energy.coupled_spin_pairs), 1e-7, 100)
+    n = g.nodes_number
+    deg = {nid: g.get_node(nid).degree for nid in g.nodes}
+    for nid in range(n):
+        em.apply_q1(W.HADAMARD, nid)
+    for step, (mix, coup) in enumerate(W.scheduler(0.2, lambda t: 1 - t, 6)):
+        for (a, b), J in zip(energy.coupled_spin_pairs, energy.coupling_amplitudes):
+            a, b = int(a), int(b)
+            em.apply_q2(W.q2_gate(J, energy.fields[a] / deg[a], energy.fields[b] / deg[b], coup), a, b)
+        for nid in range(n):
+            em.apply_q1(W.q1_gate(mix), nid)
+        close(np.stack([em.dens_q1(i) for i in range(n)]), gold["anneal/rho_history"][step], 1e-10)
+    close(np.stack([em.dens_q1(i) for i in range(n)]), gold["anneal/rho"], 1e-10)
+    assert np.abs(np.array(em.truncation_errors) - gold["anneal/truncation_errors"]).max() < 1e-10
+    assert np.abs(np.array(em.entropies) - gold["anneal/entropies"]).max() < 1e-10
+    ref_vd = gold["anneal/after_regauging"]
+    assert len(em.after_regauging_vidal_distances) == len(ref_vd)
+    assert np.abs(np.array(em.after_regauging_vidal_distances) - ref_vd).max() < 1e-10
