@@ -137,3 +137,24 @@ def test_cpu_tensors_are_rejected():
         torch.ops.dqz.apply1(0, x, torch.zeros(1, dtype=torch.int32), x)
     with pytest.raises(RuntimeError, match="CUDA tensors only"):
         T.IMPL["apply1"](0, x, torch.zeros(1, dtype=torch.int32), x)
+
+
+def test_every_operator_traces_with_fake_tensors():
+    """Under FakeTensorMode (what torch.compile and export trace with) every
+    operator accepts fake CUDA tensors and runs its fake implementation;
+    nothing executes and no GPU is needed."""
+    from torch._subclasses.fake_tensor import FakeTensorMode
+
+    real = _fake_tensors()
+    with FakeTensorMode():
+        fakes = {k: torch.empty(v.shape, dtype=v.dtype, device="cuda") for k, v in real.items()}
+        for op in T.OPS:
+            fn = T.IMPL[op]
+            code = fn.__code__
+            kwargs = dict(CALLS[op])
+            for p in code.co_varnames[:code.co_argcount]:
+                if p == "graph":
+                    kwargs[p] = 0
+                elif p not in kwargs and p in fakes:
+                    kwargs[p] = fakes["halves_gates"] if (op == "simple_update" and p == "halves") else fakes[p]
+            assert getattr(torch.ops.dqz, op)(**kwargs) is None
