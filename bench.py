@@ -389,9 +389,11 @@ def run_ours(args, world, rank, local):
                 "algorithmic_bytes_per_launch": r["edge_updates"] * bytes_per_edge_update(
                     s=16 if prec == "fp64" else 8)}
 
-    cpu_v, cores, sample = (None, None, None)
+    cpu_v, cores, sample, cpu1 = (None, None, None, None)
     if world == 1 and not args.no_cpu:
         cpu_v, cores, sample = cpu_baseline_sample(g, tensors, m, seconds=args.cpu_seconds)
+        # one host thread as well (numpy's own BLAS threads left as they are)
+        cpu1, _, sample1 = cpu_baseline_sample(g, tensors, m, seconds=min(4.0, args.cpu_seconds), threads=1)
     line = {
         "metric": METRIC, "value": rbf["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": rbf["ms_per_step"], "higher_is_better": True,
@@ -412,7 +414,8 @@ def run_ours(args, world, rank, local):
         "speedup_vs_fp64": rbf["value"] / r64["value"],
         "accuracy": acc,
         "roofline": roof(rbf, "bf16"),
-        "cpu_baseline": {"value": cpu_v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+        "cpu_baseline": {"value": cpu_v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample,
+                         "single_thread_value": cpu1},
         "e2e": {"value": rbf["e2e"], "unit": UNIT, "h2d_bytes_per_step": rbf["h2d"],
                 "d2h_bytes_per_step": rbf["d2h"]},
         "gpu_launches": rbf["launches"],
