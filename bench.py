@@ -177,6 +177,15 @@ def cpu_baseline_sample(g, tensors_c64, m, seconds=12.0, threads=None):
     return done / dt, threads, f"{done} edge-updates ({done // DEGREE} nodes' pass_through_node) in {dt:.1f}s"
 
 
+def _jax_note() -> str:
+    """Whether the reference's own JAX CPU path could be timed on this host."""
+    import importlib.util
+
+    if importlib.util.find_spec("jax") is None:
+        return "unavailable on this box (jax is not installed); the baseline is the numpy restatement"
+    return "jax importable, but the reference package does not travel here; the baseline is the numpy restatement"
+
+
 def run_reference(args, world, rank):
     if rank != 0:
         return
@@ -415,7 +424,7 @@ def run_ours(args, world, rank, local):
         "accuracy": acc,
         "roofline": roof(rbf, "bf16"),
         "cpu_baseline": {"value": cpu_v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample,
-                         "single_thread_value": cpu1},
+                         "single_thread_value": cpu1, "reference_jax_cpu": _jax_note()},
         "e2e": {"value": rbf["e2e"], "unit": UNIT, "h2d_bytes_per_step": rbf["h2d"],
                 "d2h_bytes_per_step": rbf["d2h"]},
         "gpu_launches": rbf["launches"],
