@@ -51,6 +51,12 @@ class JArray(_np.ndarray):
     def __ipow__(self, o):
         return _np.power(self, o)
 
+    def swapaxes(self, *args, axis1=None, axis2=None):
+        # JAX's method also takes its axes by keyword
+        if args:
+            return _np.ndarray.swapaxes(self, *args)
+        return _np.ndarray.swapaxes(self, axis1, axis2)
+
     @property
     def at(self):
         # x.at[idx].set(v): a copy of x with x[idx] = v (JAX's functional update)
@@ -137,7 +143,8 @@ config = _Config()
 # The PRNG stand-in reproduces the draws of this package's oracle emulator:
 # a key holds numpy's default_rng(seed); split() returns the key and its next
 # 31-bit integer (one per Vidal canonicalisation); normal(subkey, shape) is
-# default_rng(subkey).standard_normal(shape). The JAX PRNG stream itself is
+# default_rng(subkey).standard_normal(shape), uniform(subkey, shape) is
+# default_rng(subkey).uniform(size=shape). The JAX PRNG stream itself is
 # not reproduced (nothing here depends on it but the choice of start).
 RANDOM_SHIM = """
 import numpy as _np
@@ -166,11 +173,19 @@ def normal(key, shape):
     return wrap(_np.random.default_rng(int(key)).standard_normal(shape))
 
 
+def uniform(key, shape):
+    from jax.numpy import wrap
+
+    if isinstance(key, _Key):
+        raise RuntimeError("uniform() of a split subkey only")
+    return wrap(_np.random.default_rng(int(key)).uniform(size=shape))
+
+
 def _unavailable(*args, **kwargs):
     raise RuntimeError("not available under the stand-in")
 
 
-randint = uniform = _unavailable
+randint = _unavailable
 """
 
 LAX_SHIM = """
@@ -373,6 +388,7 @@ def maps_golden(ref_root):
         if gname == "lat232":
             graph_ops(D, graph, out, put, g_t, lam, rng)
     emulator(D, out)
+    exact_emulator(D, out)
     annealer(ref_root, out)
     np.savez_compressed(os.path.join(HERE, "maps_golden.npz"), **out)
     print(f"{len(out)} map arrays written")
@@ -411,6 +427,42 @@ def annealer(ref_root, out):
     out["anneal/truncation_errors"] = np.asarray(res.truncation_errors, dtype=float)
     out["anneal/entropies"] = np.asarray(res.entropies, dtype=float)
     out["anneal/after_regauging"] = np.array([float(x) for x in np.asarray(res.vidal_distances_after_regauging)])
+
+
+def exact_emulator(D, out):
+    """ExactQuantumEmulator (quantum_emulator/exact_quantum_emulator.py:11-147)
+    on a 2x3 lattice (6 qubits): a product state, two layers of seeded random
+    one-qubit unitaries on every qubit and two-qubit unitaries on every edge,
+    then measurements of two qubits with key 5. Recorded: the gates, every
+    qubit's density matrix after each layer, the state before the
+    measurements, the outcomes and the state after them."""
+    import jax.numpy as jnp_shim
+    from jax.random import PRNGKey
+
+    from dequantizer.src.quantum_emulator.exact_quantum_emulator import ExactQuantumEmulator
+
+    rng = np.random.default_rng(21)
+    lat = D.get_nd_lattice([2, 3], 2, 2, True)
+    trav = list(lat.get_traversal_iterator())
+    nodes = [el.id for el in trav if isinstance(el, D.Node)]
+    edges = [el.id for el in trav if isinstance(el, D.Edge)]
+    em = ExactQuantumEmulator(lat, PRNGKey(5))
+    bits = {n: int(i % 2) for i, n in enumerate(nodes)}
+    em.set_to_product_state(bits)
+    out["exact/nodes"] = np.array([repr(n) for n in nodes])
+    out["exact/bits"] = np.array([bits[n] for n in nodes])
+    for layer in range(2):
+        g1 = [unitary(rng, 2) for _ in nodes]
+        g2 = [unitary(rng, 4).reshape(2, 2, 2, 2) for _ in edges]
+        out[f"exact/g1_{layer}"], out[f"exact/g2_{layer}"] = np.stack(g1), np.stack(g2)
+        for n, g in zip(nodes, g1):
+            em.apply_q1(jnp_shim.wrap(g), n)
+        for e, g in zip(edges, g2):
+            em.apply_q2(jnp_shim.wrap(g), e[0], e[1])
+        out[f"exact/rho_{layer}"] = np.stack([np.asarray(em.dens_q1(n)) for n in nodes])
+    out["exact/measured"] = np.array([0, 3])
+    out["exact/outcomes"] = np.array([int(em.measure(nodes[i])) for i in (0, 3)])
+    out["exact/rho_after"] = np.stack([np.asarray(em.dens_q1(n)) for n in nodes])
 
 
 def emulator(D, out):

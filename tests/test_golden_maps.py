@@ -219,3 +219,36 @@ def test_annealer_matches(gold):
     ref_vd = gold["anneal/after_regauging"]
     assert len(em.after_regauging_vidal_distances) == len(ref_vd)
     assert np.abs(np.array(em.after_regauging_vidal_distances) - ref_vd).max() < 1e-10
+
+
+def test_exact_emulator_matches(gold):
+    """The oracle's dense-state ExactQuantumEmulator against the reference's on
+    a 2x3 lattice: a product state, two layers of random one- and two-qubit
+    unitaries (densities after each), then two measurements. The reference's
+    samples come from its key 5 (two draws per measurement, the second kept
+    only to stay in step with the BP emulator); they are recomputed here from
+    the same seeded stream."""
+    from dequantizer_b200.graph import Edge
+    from oracle.emulator import ExactQuantumEmulator
+
+    lat = G.get_nd_lattice([2, 3], 2, 2, True)
+    trav = list(lat.get_traversal_iterator())
+    nodes = [el.id for el in trav if isinstance(el, Node)]
+    edges = [el.id for el in trav if isinstance(el, Edge)]
+    assert [repr(n) for n in nodes] == [str(x) for x in gold["exact/nodes"]]
+    em = ExactQuantumEmulator(lat)
+    em.set_to_product_state({n: int(b) for n, b in zip(nodes, gold["exact/bits"])})
+    for layer in range(2):
+        for n, g in zip(nodes, gold[f"exact/g1_{layer}"]):
+            em.apply_q1(g, n)
+        for e, g in zip(edges, gold[f"exact/g2_{layer}"]):
+            em.apply_q2(g, e[0], e[1])
+        close(np.stack([em.dens_q1(n) for n in nodes]), gold[f"exact/rho_{layer}"], 1e-12)
+    stream = np.random.default_rng(5)
+    outcomes = []
+    for i in gold["exact/measured"]:
+        sample = np.random.default_rng(int(stream.integers(0, 2**31 - 1))).uniform(size=(1,))[0]
+        stream.integers(0, 2**31 - 1)
+        outcomes.append(em.measure(nodes[int(i)], sample))
+    assert outcomes == list(gold["exact/outcomes"])
+    close(np.stack([em.dens_q1(n) for n in nodes]), gold["exact/rho_after"], 1e-12)
