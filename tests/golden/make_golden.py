@@ -470,8 +470,10 @@ def emulator(D, out):
     heavy-hex cell: key 42, bond dimension <= 4, regauge after every layer of
     two-site gates (BP accuracy 1e-7, at most 100 iterations), three layers
     of RX(0.8) on every qubit and RZZ(-pi/2) on every edge in traversal order.
-    Recorded: every qubit's density matrix after each layer, and the
-    emulator's truncation errors, entropies and Vidal distances."""
+    Then two measurements (samples from the stand-in PRNG, re-canonicalisation
+    after each). Recorded: every qubit's density matrix after each layer and
+    after the measurements, the outcomes, and the emulator's truncation
+    errors, entropies and Vidal distances."""
     import jax.numpy as jnp_shim
     from jax.random import PRNGKey
 
@@ -489,6 +491,9 @@ def emulator(D, out):
             if isinstance(el, D.Edge):
                 em.apply_q2(rzz, *el.id)
         out[f"emu/rho_{layer}"] = np.stack([np.asarray(em.dens_q1(n)) for n in nodes])
+    out["emu/measured"] = np.array([0, 2])
+    out["emu/outcomes"] = np.array([int(em.measure(nodes[i])) for i in (0, 2)])
+    out["emu/rho_after_measure"] = np.stack([np.asarray(em.dens_q1(n)) for n in nodes])
     out["emu/truncation_errors"] = np.array([float(x) for x in em.truncation_errors])
     out["emu/entropies"] = np.array([float(x) for x in em.entropies])
     out["emu/after_regauging"] = np.array([float(x) for x in np.asarray(em.after_regauging_vidal_distances)])

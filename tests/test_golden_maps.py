@@ -163,8 +163,8 @@ def test_emulator_matches(gold):
     """The oracle's BPQuantumEmulator against the reference's on the infinite
     heavy-hex cell (key 42, bond <= 4, regauge per layer, three kicked-Ising
     layers; the reference's initial messages drawn as the oracle draws them):
-    every qubit's density matrix after each layer, truncation errors,
-    entropies and Vidal distances."""
+    every qubit's density matrix after each layer and after two measurements,
+    the outcomes, truncation errors, entropies and Vidal distances."""
     from dequantizer_b200.graph import Edge
     from oracle.emulator import BPQuantumEmulator as OracleEmulator
 
@@ -182,6 +182,15 @@ def test_emulator_matches(gold):
             if isinstance(el, Edge):
                 em.apply_q2(rzz, *el.id)
         close(np.stack([em.dens_q1(n) for n in nodes]), gold[f"emu/rho_{layer}"], 1e-10)
+    # the reference draws each sample from its key stream, then re-canonicalises
+    # with the next seed; the oracle takes the sample as an argument, so the
+    # sample's seed is drawn from its generator first to keep both in step
+    outcomes = []
+    for i in gold["emu/measured"]:
+        sample = np.random.default_rng(int(em._rng.integers(0, 2**31 - 1))).uniform(size=(1,))[0]
+        outcomes.append(em.measure(nodes[int(i)], sample))
+    assert outcomes == list(gold["emu/outcomes"])
+    close(np.stack([em.dens_q1(n) for n in nodes]), gold["emu/rho_after_measure"], 1e-10)
     assert len(em.truncation_errors) == len(gold["emu/truncation_errors"])
     assert np.abs(np.array(em.truncation_errors) - gold["emu/truncation_errors"]).max() < 1e-10
     assert np.abs(np.array(em.entropies) - gold["emu/entropies"]).max() < 1e-10
