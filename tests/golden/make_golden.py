@@ -301,6 +301,25 @@ def main(ref_root):
     shared = np.sort(np.abs(rng.standard_normal(4)))[::-1] + 0.05
     lam1 = [np.abs(rng.standard_normal(2)) + 0.1, np.abs(rng.standard_normal(3)) + 0.1, shared]
     lam2 = [shared, np.abs(rng.standard_normal(3)) + 0.1]
+    # the production shapes: a degree-3 node with bonds of dimension 16 (the
+    # mixed-precision benchmark) and a simple update between degree-3 nodes
+    # with bonds of dimension 8 under a rank cap of 8 (batched annealing)
+    rng16 = np.random.default_rng(16)
+    t = crandn(rng16, 16, 16, 16, 2) / 64
+    msgs = [psd(rng16, 16) for _ in range(3)]
+    put("ptn_k3_chi16", "tensor", t)
+    put("ptn_k3_chi16", "msg", msgs)
+    put("ptn_k3_chi16", "out", R.pass_through_node(cp(t), cp(msgs)))
+    t8a, t8b = crandn(rng16, 8, 8, 8, 2), crandn(rng16, 8, 8, 8, 2)
+    sh8 = np.sort(np.abs(rng16.standard_normal(8)))[::-1] + 0.01
+    l8a = [np.abs(rng16.standard_normal(8)) + 0.01, np.abs(rng16.standard_normal(8)) + 0.01, sh8]
+    l8b = [sh8, np.abs(rng16.standard_normal(8)) + 0.01, np.abs(rng16.standard_normal(8)) + 0.01]
+    res = R.simple_update(cp(t8a), cp(t8b), cp(l8a), cp(l8b), cp(h1), cp(h2), 2, 0, 1e-10, None, 8)
+    put("su_chi8", "t", [t8a, t8b])
+    put("su_chi8", "lam1", l8a)
+    put("su_chi8", "lam2", l8b)
+    put("su_chi8", "half", [h1, h2])
+    put("su_chi8", "out", [res[0], res[1], res[2], np.array(res[3]), np.array(res[4])])
     for case, acc, rank in [("su_acc", 1e-2, None), ("su_rank", None, 3)]:
         res = R.simple_update(cp(t1), cp(t2), cp(lam1), cp(lam2), cp(h1), cp(h2), 2, 0, 1e-10, acc, rank)
         put(case, "t", [t1, t2])

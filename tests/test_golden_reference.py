@@ -36,7 +36,7 @@ def close(a, b, tol=TOL):
     assert np.abs(a - b).max() <= tol * scale
 
 
-@pytest.mark.parametrize("case", ["ptn_k2", "ptn_k3", "ptn_k4", "ptn_k3_d3"])
+@pytest.mark.parametrize("case", ["ptn_k2", "ptn_k3", "ptn_k4", "ptn_k3_d3", "ptn_k3_chi16"])
 def test_pass_through_node(g, case):
     out = OT.pass_through_node(g[f"{case}/tensor"], lst(g, f"{case}/msg"))
     for a, b in zip(out, lst(g, f"{case}/out")):
@@ -75,7 +75,7 @@ def test_apply_half_gate(g):
     close(OT.apply_half_gate(g["ahg/tensor"], h1, 1), g["ahg/out"])
 
 
-@pytest.mark.parametrize("case,acc,rank", [("su_acc", 1e-2, None), ("su_rank", None, 3)])
+@pytest.mark.parametrize("case,acc,rank", [("su_acc", 1e-2, None), ("su_rank", None, 3), ("su_chi8", None, 8)])
 def test_simple_update(g, case, acc, rank):
     t1, t2 = lst(g, f"{case}/t")
     h1, h2 = lst(g, f"{case}/half")
