@@ -199,3 +199,17 @@ def test_umma_layout_model_bf16_error_bound(seed):
     for e in range(3):
         err = np.abs(got[e] - ref[e]).max() / np.abs(ref[e]).max()
         assert 1e-5 < err < 3e-2
+
+
+def test_umma_layout_model_matches_reference_golden():
+    """The modelled kernel data flow on the reference's own recorded
+    pass_through_node at this shape (tests/golden, degree 3, bonds 16)."""
+    import os
+
+    g = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "tensor_ops_golden.npz"))
+    T = g["ptn_k3_chi16/tensor"]
+    msgs = [g[f"ptn_k3_chi16/msg{i}"] for i in range(3)]
+    got = model_node_update(T, msgs, lambda x: np.asarray(x, dtype=np.float64))
+    for e in range(3):
+        ref = g[f"ptn_k3_chi16/out{e}"]
+        assert np.abs(got[e] - ref).max() < 1e-12 * np.abs(ref).max()
