@@ -6,11 +6,14 @@ the reference's synchronous mode (one node-update launch + one edge pass).
 ``value`` is timed on the device with CUDA events per step, inputs resident
 in HBM, L2 flushed (a 512 MB write) between steps outside the timed events.
 ``e2e`` is the same sweep through the public engine API with host buffers:
-pinned complex64 node tensors and complex128 messages copied in, the sweep,
-the node->edge messages copied back, all inside the timed region.
+pinned complex64 node tensors and messages copied in, the sweep, the
+node->edge messages copied back, all inside the timed region
+(``BPEngine.sweep_host``: the copies stream in node ranges that are packed
+and updated as they arrive, overlapping the transfers with the kernels).
 
 ``--impl reference`` times the CPU restatement of the reference algorithm
-(numpy FP64, threads over nodes) on a bounded sample of the same workload.
+(numpy FP64 pass_through_node, one process per host core with one BLAS thread
+each) on a bounded sample of the same workload.
 With torchrun (N > 1) every rank runs an independent replica ("replicas
 only": the sweep of one graph has no exchange step here).
 """
@@ -151,30 +154,79 @@ def barrier(world: int):
         dist.barrier()
 
 
-def cpu_baseline_sample(g, tensors_c64, m, seconds=12.0, threads=None):
-    """Oracle pass_through_node over nodes (threads over nodes), on the host
-    cores, for about ``seconds``; returns (edge-updates/s, threads, sample)."""
-    from concurrent.futures import ThreadPoolExecutor
+CPU_SAMPLE_NODES = 64  # node tensors each CPU worker cycles through (4 MB of complex64)
 
+
+def _cpu_worker_init():
+    from threadpoolctl import threadpool_limits
+
+    threadpool_limits(1)  # one BLAS thread per worker process: the pool supplies the parallelism
+
+
+def _cpu_worker(args):
+    """One worker: the oracle's pass_through_node (complex128) over its share
+    of the sampled node tensors for ``seconds``; returns (node updates, seconds)."""
+    tensors, m, seconds, start = args
     from oracle import tensor_ops as OT
 
-    threads = threads or os.cpu_count() or 1
-    nodes = list(g.nodes.values())
     shape = (CHI,) * DEGREE + (PHYS,)
     msgs = [m] * DEGREE
+    t64 = [t.astype(np.complex128).reshape(shape) for t in tensors]
+    done, i = 0, start
+    t0 = time.perf_counter()
+    while time.perf_counter() - t0 < seconds:
+        OT.pass_through_node(t64[i % len(t64)], msgs)
+        done += 1
+        i += 1
+    return done, time.perf_counter() - t0
 
-    def work(v):
-        OT.pass_through_node(tensors_c64[v].astype(np.complex128).reshape(shape), msgs)
-        return DEGREE
 
-    done, t0, v = 0, time.perf_counter(), 0
-    with ThreadPoolExecutor(max_workers=threads) as ex:
-        while time.perf_counter() - t0 < seconds:
-            batch = [(v + i) % len(nodes) for i in range(threads * 4)]
-            v += len(batch)
-            done += sum(ex.map(work, batch))
-    dt = time.perf_counter() - t0
-    return done / dt, threads, f"{done} edge-updates ({done // DEGREE} nodes' pass_through_node) in {dt:.1f}s"
+class CpuBaseline:
+    """The oracle's pass_through_node on the host cores: ``procs`` worker
+    processes (default: every core), started with spawn and limited to one
+    BLAS thread each, every one cycling over the same sample of
+    CPU_SAMPLE_NODES node tensors. The pool starts once; ``sample(seconds)``
+    returns (edge-updates/s summed over the workers, workers, description)."""
+
+    def __init__(self, tensors_c64, m, procs=None):
+        import multiprocessing as mp
+
+        self.procs = procs or os.cpu_count() or 1
+        self.sample_t = np.ascontiguousarray(tensors_c64[:CPU_SAMPLE_NODES])
+        self.m = m
+        old = os.environ.get("OPENBLAS_NUM_THREADS")
+        os.environ["OPENBLAS_NUM_THREADS"] = "1"
+        try:
+            self.pool = mp.get_context("spawn").Pool(self.procs, initializer=_cpu_worker_init)
+        finally:
+            if old is None:
+                os.environ.pop("OPENBLAS_NUM_THREADS", None)
+            else:
+                os.environ["OPENBLAS_NUM_THREADS"] = old
+        self.pool.map(_cpu_worker, [(self.sample_t[:2], m, 0.2, 0)] * self.procs)  # imports, untimed
+
+    def sample(self, seconds):
+        res = self.pool.map(_cpu_worker, [(self.sample_t, self.m, seconds, k) for k in range(self.procs)])
+        rate = sum(DEGREE * n / dt for n, dt in res)
+        nodes = sum(n for n, _ in res)
+        return rate, self.procs, (f"{self.procs} processes x 1 BLAS thread, {nodes} nodes' pass_through_node "
+                                  f"({DEGREE * nodes} edge-updates) in ~{seconds:.0f}s, cycling over "
+                                  f"{len(self.sample_t)} of the workload's node tensors")
+
+    @staticmethod
+    def single(tensors_c64, m, seconds):
+        with CpuBaseline(tensors_c64, m, procs=1) as one:
+            return one.sample(seconds)
+
+    def close(self):
+        self.pool.close()
+        self.pool.join()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
 
 
 def _jax_note() -> str:
@@ -190,12 +242,14 @@ def run_reference(args, world, rank):
     if rank != 0:
         return
     g, tensors, m = workload(0)
-    for _ in range(args.warmup):
-        cpu_baseline_sample(g, tensors, m, seconds=1.0)
     vals = []
-    for _ in range(args.steps):
-        v, threads, sample = cpu_baseline_sample(g, tensors, m, seconds=args.ref_seconds)
-        vals.append(v)
+    with CpuBaseline(tensors, m) as cpu:
+        for _ in range(args.warmup):
+            cpu.sample(0.5)
+        for _ in range(args.steps):
+            v, threads, sample = cpu.sample(args.ref_seconds)
+            vals.append(v)
+        single, _, _ = CpuBaseline.single(tensors, m, min(2.0, args.ref_seconds))
     value = float(np.mean(vals))
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
@@ -204,8 +258,8 @@ def run_reference(args, world, rank):
         "config": {"workload": "random 3-regular graph, 1024 nodes, chi=16, d=2: one synchronous BP sweep "
                    "(3072 edge-updates)", "sample_per_step": f"~{args.ref_seconds:.0f}s of node updates"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-                         "sample": "numpy FP64 restatement of tensor_ops.pass_through_node, threads over nodes, "
-                                   + sample},
+                         "sample": "numpy FP64 restatement of tensor_ops.pass_through_node, "
+                                   + sample, "single_process_value": single},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -282,10 +336,7 @@ def time_engine(args, world, g, packed_c64, m, precision, flush, clk=None):
         flush.zero_()
         s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         s.record(stream)
-        eng.load_tensors_host(packed_c64)
-        eng.load_messages_host(n2e_host, e2n_host)
-        eng.sweep()
-        eng.read_messages_host(out_host)
+        eng.sweep_host(packed_c64, n2e_host, e2n_host, out_host, chunks=args.e2e_chunks)
         e.record(stream)
         e.synchronize()
         e_times.append(s.elapsed_time(e) * 1e-3)
@@ -307,50 +358,131 @@ def time_engine(args, world, g, packed_c64, m, precision, flush, clk=None):
     }
 
 
-def accuracy_check(g, packed_c64, m, tol=1e-6, max_sweeps=400):
-    """BP from the same start: FP64 sweeps to the tolerance, then the same
-    number of FP32 and BF16 sweeps (BF16 sweeps settle at their rounding
-    floor, about 1e-4 in message distance, rather than at ``tol``); max
-    |<Z_i>| difference of the one-site density matrices, all read out in FP64."""
+def packed_inputs(g, tensors):
+    """Node tensors in the engine's node order (DFS traversal), flattened."""
+    import torch
+
+    from dequantizer_b200.maps import Topology
+
+    topo = Topology(list(g.get_traversal_iterator(ordering="dfs")), True)
+    pos = {nid: i for i, nid in enumerate(g.nodes.keys())}
+    perm = np.array([pos[n.id] for n in topo.nodes])
+    return torch.from_numpy(np.ascontiguousarray(tensors[perm]).reshape(-1)).pin_memory()
+
+
+def convergence_study(seeds=(0, 1, 2), tol=1e-6, max_sweeps=400, bf16_tol=2e-4):
+    """BP run to a message distance of ``tol`` from the same start in each
+    form, then the Vidal gauge and the one-site densities (all FP64 on the
+    final messages), for several seeds of the bench workload:
+    * fp64: FP64 sweeps to ``tol``;
+    * fp32: FP32 sweeps to ``tol``;
+    * mixed: BF16 tensor-core sweeps to ``bf16_tol`` (above their rounding
+      floor of ~5e-5), then an FP32 refinement tail to ``tol``.
+    Per form: sweeps, device time to the tolerance (CUDA events around the
+    loop, distance read back every sweep), and against FP64 the largest
+    |delta lambda| over all bond spectra, the largest |delta rho_i| entry over
+    all one-site densities and the largest |delta <Z_i>|."""
     import torch
 
     from dequantizer_b200.engine import BPEngine
 
-    out, iters = {}, None
-    for prec in ("fp64", "fp32", "bf16"):
+    def engine(g, prec, packed, m):
+        eng = BPEngine(g, traversal="dfs", schedule="sync", precision=prec)
+        mdt = torch.complex128 if prec == "fp64" else torch.complex64
+        msgs = torch.from_numpy(np.tile(m.reshape(-1), eng.layout.n_halves)).to(mdt)
+        eng.load_tensors_host(packed)
+        eng.load_messages_host(msgs, msgs)
+        return eng
+
+    def timed(fn):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        s.record()
+        out = fn()
+        e.record()
+        e.synchronize()
+        return out, s.elapsed_time(e)
+
+    def observables(eng):
+        _, lam = eng.vidal_gauge(1e-10)
+        rho = eng.densities()
+        z = (rho[:, 0, 0] - rho[:, 1, 1]).real
+        return lam, rho, z
+
+    per_seed = []
+    for seed in seeds:
+        g, tensors, m = workload(seed)
+        packed = packed_inputs(g, tensors)
+        res = {}
+        e64 = engine(g, "fp64", packed, m)
+        n64, t64 = timed(lambda: e64.run(tol, max_sweeps))
+        ref = observables(e64)
+        res["fp64"] = {"sweeps": n64, "ms": t64, "final_distance": float(e64.distance())}
+        e32 = engine(g, "fp32", packed, m)
+        n32, t32 = timed(lambda: e32.run(tol, max_sweeps))
+        res["fp32"] = {"sweeps": n32, "ms": t32, "final_distance": float(e32.distance()), "obs": observables(e32)}
+        ebf = engine(g, "bf16", packed, m)
+        ebf.sweep()  # BF16 layouts packed and kernel attributes set outside the timed loop
+        ebf.load_messages_host(torch.from_numpy(np.tile(m.reshape(-1), ebf.layout.n_halves)).to(torch.complex64),
+                               torch.from_numpy(np.tile(m.reshape(-1), ebf.layout.n_halves)).to(torch.complex64))
+        etail = engine(g, "fp32", packed, m)
+
+        def mixed():
+            nb = ebf.run(bf16_tol, max_sweeps)
+            etail.n2e.copy_(ebf.n2e)
+            etail.e2n.copy_(ebf.e2n)
+            nt = etail.run(tol, max_sweeps)
+            return nb, nt
+
+        (nb, nt), tm = timed(mixed)
+        res["mixed"] = {"sweeps_bf16": nb, "sweeps_fp32_tail": nt, "ms": tm,
+                        "final_distance": float(etail.distance()), "obs": observables(etail)}
+        for k in ("fp32", "mixed"):
+            lam, rho, z = res[k].pop("obs")
+            res[k]["max_abs_dlambda"] = float((lam - ref[0]).abs().max())
+            res[k]["max_abs_drho"] = float((rho - ref[1]).abs().max())
+            res[k]["max_abs_dZ"] = float((z - ref[2]).abs().max())
+        per_seed.append(res)
+    worst = lambda k, q: max(r[k][q] for r in per_seed)  # noqa: E731
+    mean = lambda k, q: float(np.mean([r[k][q] for r in per_seed]))  # noqa: E731
+    out = {"tol": tol, "bf16_handover_tol": bf16_tol, "seeds": list(seeds), "bound_dZ": 1e-4,
+           "per_seed": per_seed}
+    for k in ("fp32", "mixed"):
+        out[k] = {q: worst(k, q) for q in ("max_abs_dlambda", "max_abs_drho", "max_abs_dZ")}
+        out[k]["ok"] = out[k]["max_abs_dZ"] <= 1e-4
+    for k in ("fp64", "fp32", "mixed"):
+        out.setdefault(k, {})["mean_ms_to_tol"] = mean(k, "ms")
+    out["time_to_tol_speedup_mixed_vs_fp64"] = out["fp64"]["mean_ms_to_tol"] / out["mixed"]["mean_ms_to_tol"]
+    out["time_to_tol_speedup_fp32_vs_fp64"] = out["fp64"]["mean_ms_to_tol"] / out["fp32"]["mean_ms_to_tol"]
+    return out
+
+
+def bf16_sweep_accuracy(g, packed_c64, m, sweeps):
+    """The per-sweep claim: the same number of BF16 tensor-core sweeps as FP64
+    needs for the tolerance, from the same start; max |delta <Z_i>| against FP64."""
+    import torch
+
+    from dequantizer_b200.engine import BPEngine
+
+    z = {}
+    for prec in ("fp64", "bf16"):
         eng = BPEngine(g, traversal="dfs", schedule="sync", precision=prec)
         mdt = torch.complex128 if prec == "fp64" else torch.complex64
         msgs = torch.from_numpy(np.tile(m.reshape(-1), eng.layout.n_halves)).to(mdt)
         eng.load_tensors_host(packed_c64)
         eng.load_messages_host(msgs, msgs)
-        if iters is None:
-            iters = eng.run(tol, max_sweeps=max_sweeps, check_every=5)
-        else:
-            for _ in range(iters):
-                eng.sweep()
+        for _ in range(sweeps):
+            eng.sweep()
         rho = eng.densities()
-        z = (rho[:, 0, 0] - rho[:, 1, 1]).real.double().cpu().numpy()
-        out[prec] = (z, float(eng.distance()))
-    res = {"bound": 1e-4, "tol_fp64": tol, "sweeps": iters}
-    for prec in ("fp32", "bf16"):
-        dz = float(np.abs(out["fp64"][0] - out[prec][0]).max())
-        res[prec] = {"max_abs_dZ": dz, "ok": dz <= 1e-4, "final_distance": out[prec][1]}
-    res["final_distance_fp64"] = out["fp64"][1]
-    res["max_abs_dZ"] = res["bf16"]["max_abs_dZ"]
-    res["ok"] = res["bf16"]["ok"]
-    return res
+        z[prec] = (rho[:, 0, 0] - rho[:, 1, 1]).real
+    return float((z["bf16"] - z["fp64"]).abs().max())
 
 
 def run_ours(args, world, rank, local):
     import torch
 
     g, tensors, m = workload(rank)
-    from dequantizer_b200.maps import Topology
-
-    topo = Topology(list(g.get_traversal_iterator(ordering="dfs")), True)
-    pos = {nid: i for i, nid in enumerate(g.nodes.keys())}
-    perm = np.array([pos[n.id] for n in topo.nodes])
-    packed_c64 = torch.from_numpy(np.ascontiguousarray(tensors[perm]).reshape(-1)).pin_memory()
+    packed_c64 = packed_inputs(g, tensors)
     flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
     precs = [args.only] if args.only else ["fp64", "fp32", "bf16"]
@@ -364,7 +496,11 @@ def run_ours(args, world, rank, local):
             print(json.dumps({"only": args.only, "value": r["value"], "node_ms": r["node_ms"],
                               "kernel": r["kernel"], "e2e": r["e2e"]}), flush=True)
         return
-    acc = accuracy_check(g, packed_c64, m) if not args.no_accuracy else None
+    acc = None
+    if not args.no_accuracy:
+        acc = convergence_study()
+        acc["bf16_same_sweeps_max_abs_dZ"] = bf16_sweep_accuracy(g, packed_c64, m,
+                                                                  acc["per_seed"][0]["fp64"]["sweeps"])
     peaks = {}
     if rank == 0:
         peaks["fp64"] = measure_peak(torch, torch.float64)
@@ -400,9 +536,10 @@ def run_ours(args, world, rank, local):
 
     cpu_v, cores, sample, cpu1 = (None, None, None, None)
     if world == 1 and not args.no_cpu:
-        cpu_v, cores, sample = cpu_baseline_sample(g, tensors, m, seconds=args.cpu_seconds)
-        # one host thread as well (numpy's own BLAS threads left as they are)
-        cpu1, _, sample1 = cpu_baseline_sample(g, tensors, m, seconds=min(4.0, args.cpu_seconds), threads=1)
+        with CpuBaseline(tensors, m) as cpu:
+            cpu_v, cores, sample = cpu.sample(args.cpu_seconds)
+        # one worker process with one BLAS thread: the single-core figure
+        cpu1, _, _ = CpuBaseline.single(tensors, m, min(4.0, args.cpu_seconds))
     line = {
         "metric": METRIC, "value": rbf["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": rbf["ms_per_step"], "higher_is_better": True,
@@ -424,7 +561,7 @@ def run_ours(args, world, rank, local):
         "accuracy": acc,
         "roofline": roof(rbf, "bf16"),
         "cpu_baseline": {"value": cpu_v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample,
-                         "single_thread_value": cpu1, "reference_jax_cpu": _jax_note()},
+                         "single_process_value": cpu1, "reference_jax_cpu": _jax_note()},
         "e2e": {"value": rbf["e2e"], "unit": UNIT, "h2d_bytes_per_step": rbf["h2d"],
                 "d2h_bytes_per_step": rbf["d2h"]},
         "gpu_launches": rbf["launches"],
@@ -654,8 +791,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
-    ap.add_argument("--ref-seconds", type=float, default=8.0)
+    ap.add_argument("--ref-seconds", type=float, default=4.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--e2e-chunks", type=int, default=8,
+                    help="node ranges the end-to-end sweep streams its host inputs in (1: no overlap)")
     ap.add_argument("--no-accuracy", action="store_true")
     ap.add_argument("--only", choices=["fp64", "fp32", "bf16"], default=None,
                     help="time one precision only (profiling runs); prints a short line")

@@ -85,6 +85,7 @@ _SIGNATURES = {
     "dqz_bp_node_update_k3_umma": (ctypes.c_int, [_G, _P, _P, _P, _P, _P, _P, _I, _P, _P]),
     "dqz_bf16_umma_elems_per_node": (_S, []),
     "dqz_pack_bf16_umma": (ctypes.c_int, [_G, _P, _P, _P]),
+    "dqz_pack_bf16_umma_nodes": (ctypes.c_int, [_G, _P, _P, _I, _I, _P]),
     "dqz_pack_bf16_planes": (ctypes.c_int, [_G, _P, _P, _P]),
     "dqz_messages_distance": (ctypes.c_int, [_G, _P, _P, _P, _P, _P, _P, _I, _P]),
     "dqz_reduce_sum": (ctypes.c_int, [_P, _I, _D, _P, _P]),
@@ -117,6 +118,7 @@ _SIGNATURES = {
     "dqz_simple_update_scratch_bytes": (_S, [_I, _I, _I]),
     "dqz_simple_update_noalloc": (ctypes.c_int, [_G, _P, _P, _P, _P, _P, _P, _I, _D, _I, _I, _I, _P, _P, _P]),
     "dqz_repack": (ctypes.c_int, [_P, _P, _P, _P, _P, _I, _I, _P]),
+    "dqz_count_nonfinite": (ctypes.c_int, [_P, ctypes.c_int64, _I, _P, _P]),
 }
 
 _lib: Optional[ctypes.CDLL] = None
@@ -168,6 +170,26 @@ def require_cuda(*tensors: torch.Tensor):
                 "dequantizer_b200 runs on the GPU only: expected CUDA tensors "
                 f"(got {type(t).__name__} on {getattr(t, 'device', 'host')})"
             )
+
+
+class NonFiniteError(DqzError):
+    """NaN or Inf met in the state of a BP loop (status DQZ_ERR_NONFINITE)."""
+
+    def __init__(self, where: str):
+        super().__init__(where, DQZ_ERR_NONFINITE)
+
+
+def count_nonfinite(t: torch.Tensor) -> int:
+    """Number of NaN / Inf real words in a CUDA tensor (complex entries count
+    their real and imaginary parts); synchronises with the stream."""
+    require_cuda(t)
+    t = t.contiguous()
+    real = torch.view_as_real(t) if t.is_complex() else t
+    if real.dtype not in (torch.float64, torch.float32):
+        raise TypeError(f"count_nonfinite takes float32/64 or complex64/128 tensors, not {t.dtype}")
+    cnt = torch.zeros(1, dtype=torch.int32, device=t.device)
+    call("dqz_count_nonfinite", real.data_ptr(), real.numel(), real.element_size(), cnt.data_ptr(), stream_handle())
+    return int(cnt.item())
 
 
 def device() -> torch.device:

@@ -604,11 +604,12 @@ done:
 
 // T (complex64, node v at node_off[v], [a][b][c][s]) -> Tu (BF16, node v at
 // v * NODE_ELEMS, [s][L1 re, L1 im, L2 re, L2 im][4096]).
-__global__ void pack_bf16_umma_kernel(dqz_graph_t g, const float2 *__restrict__ T, __nv_bfloat16 *Tu) {
+__global__ void pack_bf16_umma_kernel(dqz_graph_t g, const float2 *__restrict__ T, __nv_bfloat16 *Tu, int first,
+                                      int count) {
   const int per = 4096;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < (long long)g.n_nodes * per;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < (long long)count * per;
        i += (long long)gridDim.x * blockDim.x) {
-    const int v = (int)(i / per), x = (int)(i % per);
+    const int v = first + (int)(i / per), x = (int)(i % per);
     const int a = x >> 8, b = (x >> 4) & 15, c = x & 15;
     const float2 *t = T + g.node_off[v] + 2 * x;
     const int o1 = off_l1(a, b, c), o2 = off_l2(a, b, c);
@@ -633,7 +634,21 @@ extern "C" int dqz_pack_bf16_umma(const dqz_graph_t *g, const void *tensors_c64,
   if (!g || !tensors_c64 || !tensors_bf16) return DQZ_ERR_ARG;
   if (((uintptr_t)tensors_bf16 & 15) != 0) return DQZ_ERR_ARG;
   if (g->n_nodes == 0) return DQZ_OK;
-  pack_bf16_umma_kernel<<<148 * 8, 256, 0, stream>>>(*g, (const float2 *)tensors_c64, (__nv_bfloat16 *)tensors_bf16);
+  pack_bf16_umma_kernel<<<148 * 8, 256, 0, stream>>>(*g, (const float2 *)tensors_c64, (__nv_bfloat16 *)tensors_bf16,
+                                                     0, g->n_nodes);
+  DQZ_CHECK_LAUNCH();
+  return DQZ_OK;
+}
+
+extern "C" int dqz_pack_bf16_umma_nodes(const dqz_graph_t *g, const void *tensors_c64, void *tensors_bf16,
+                                        int32_t first, int32_t count, cudaStream_t stream) {
+  if (!g || !tensors_c64 || !tensors_bf16 || first < 0 || count < 0 || first + count > g->n_nodes) return DQZ_ERR_ARG;
+  if (((uintptr_t)tensors_bf16 & 15) != 0) return DQZ_ERR_ARG;
+  if (count == 0) return DQZ_OK;
+  const long long blocks = ((long long)count * 4096 + 255) / 256;
+  const int grid = (int)(blocks < 148 * 8 ? blocks : 148 * 8);
+  pack_bf16_umma_kernel<<<grid, 256, 0, stream>>>(*g, (const float2 *)tensors_c64, (__nv_bfloat16 *)tensors_bf16,
+                                                  first, count);
   DQZ_CHECK_LAUNCH();
   return DQZ_OK;
 }

@@ -79,3 +79,31 @@ extern "C" int dqz_repack(const void *src, void *dst, const int64_t *src_off, co
   DQZ_CHECK_LAUNCH();
   return DQZ_OK;
 }
+
+namespace {
+
+// Grid-stride count of non-finite words (NaN or +-Inf); one atomic per warp.
+template <typename F>
+__global__ void count_nonfinite_kernel(const F *x, int64_t n, int32_t *count) {
+  int local = 0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    local += isfinite(x[i]) ? 0 : 1;
+  local = __reduce_add_sync(0xffffffffu, local);
+  if ((threadIdx.x & 31) == 0 && local) atomicAdd(count, local);
+}
+
+}  // namespace
+
+extern "C" int dqz_count_nonfinite(const void *data, int64_t n, int32_t elem_bytes, int32_t *count,
+                                   cudaStream_t stream) {
+  if (!data || !count || n < 0 || (elem_bytes != 4 && elem_bytes != 8)) return DQZ_ERR_ARG;
+  if (n == 0) return DQZ_OK;
+  const int64_t blocks = (n + 255) / 256;
+  const int grid = (int)(blocks < 148 * 8 ? blocks : 148 * 8);
+  if (elem_bytes == 8)
+    count_nonfinite_kernel<double><<<grid, 256, 0, stream>>>((const double *)data, n, count);
+  else
+    count_nonfinite_kernel<float><<<grid, 256, 0, stream>>>((const float *)data, n, count);
+  DQZ_CHECK_LAUNCH();
+  return DQZ_OK;
+}

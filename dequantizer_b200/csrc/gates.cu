@@ -438,9 +438,9 @@ extern "C" int dqz_simple_update_noalloc(const dqz_graph_t *g, void *tensors, do
   size_t slots = (size_t)DQZ_NOALLOC_SCRATCH_BYTES / per_job;
   int grid = n < SU_GRID_MAX ? n : SU_GRID_MAX;
   if ((size_t)grid > slots) grid = (int)slots;
-  if (cudaFuncSetAttribute(simple_update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_LIMIT) !=
-      cudaSuccess)
-    return DQZ_ERR_CUDA;
+  const int tuned = dqz_get_tuning(DQZ_TUNE_SU_GRID);  // the tuned grid, never above the slices
+  if (tuned > 0 && tuned < grid) grid = tuned;
+  DQZ_SMEM_ATTR_ONCE(simple_update_kernel, SMEM_LIMIT);
   simple_update_kernel<<<grid, GATE_THREADS, smem, stream>>>(*g, (cd *)tensors, lambdas, edges, ctrl_is_first,
                                                              (const cd *)halves, ranks, n, eps, max_rank, max_rows,
                                                              max_cols, err, entropy, (cd *)scratch);

@@ -15,6 +15,7 @@ and one simple-update launch.
 """
 
 import logging
+import math
 from typing import Dict, List, Optional
 
 import numpy as np
@@ -355,7 +356,14 @@ class BPQuantumEmulator:
     def _bp_loop(self, T, n2e, e2n, vd, G, lam):
         L = self._layout
         iters = 0
-        while float(vd) > self.accuracy:
+        while True:
+            d = float(vd)
+            if not math.isfinite(d):
+                # the reference's loop stops here too (NaN > accuracy is false) but
+                # keeps the NaN state silently; this one reports it
+                raise _lib.NonFiniteError(f"BP regauge iteration {iters}: Vidal distance {d}")
+            if d <= self.accuracy:
+                break
             if self.max_iters is not None and self.max_iters <= iters:
                 log.warning("Belief propagation reached the maximal number of iterations.")
                 break

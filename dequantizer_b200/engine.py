@@ -10,7 +10,10 @@ and exposes whole-graph operations on them:
 * ``distance()``         -- mean Frobenius distance between the last two
   message sets (mappings/messages_distance.py:14-22);
 * ``run()``              -- sweeps to a tolerance, like the reference's
-  driver loops (examples/3d_ising_canonicalization.py:137-145);
+  driver loops (examples/3d_ising_canonicalization.py:137-145); at the sweep
+  cap it logs the reference's warning (bp_quantum_emulator.py:288-291) and
+  sets ``status`` to DQZ_ERR_NOT_CONVERGED; a NaN / Inf distance raises
+  ``NonFiniteError`` (DQZ_ERR_NONFINITE);
 * ``vidal_gauge()`` / ``vidal_distance()`` / ``densities()`` (FP64).
 
 ``precision="fp64"`` keeps complex128 arenas (the plain form);
@@ -21,7 +24,9 @@ Host arrays are loaded and read back through the ``*_host`` methods, the
 end-to-end path.
 """
 
-from typing import List, Optional, Sequence
+import logging
+import math
+from typing import Callable, List, Optional, Sequence
 
 import numpy as np
 import torch
@@ -31,8 +36,33 @@ from .graph import TensorGraph
 from .layout import GraphLayout
 from .maps import BF16_KERNELS, Topology, bp_sweep, density_packed, error_flag, vidal_distance_packed, vidal_gauge_packed
 
+log = logging.getLogger(__name__)
+
 SCHEDULES = ("sync", "async", "flooding")
-PRECISIONS = {"fp64": torch.complex128, "fp32": torch.complex64, "bf16": torch.complex64}
+
+
+def converge(step: Callable[[], None], distance: Callable[[], float], tol: float, max_sweeps: int,
+             sweeps_per_step: int = 1, first: int = 0):
+    """The stopping rule shared by the BP loops: ``step()`` advances
+    ``sweeps_per_step`` sweeps, ``distance()`` reads the distance after it.
+    Returns (sweeps done, status): DQZ_OK once the distance is <= tol,
+    DQZ_ERR_NOT_CONVERGED at the cap (with the reference's warning). A NaN or
+    Inf distance raises NonFiniteError: the reference's loop would stop there
+    with a NaN state (NaN > tol is false), silently."""
+    done = first
+    while done < max_sweeps:
+        step()
+        done += sweeps_per_step
+        d = float(distance())
+        if not math.isfinite(d):
+            raise _lib.NonFiniteError(f"BP sweep {done}: message distance {d}")
+        if d <= tol:
+            return done, _lib.DQZ_OK
+    log.warning("Belief propagation reached the maximal number of iterations.")
+    return done, _lib.DQZ_ERR_NOT_CONVERGED
+
+
+PRECISIONS ={"fp64": torch.complex128, "fp32": torch.complex64, "bf16": torch.complex64}
 
 
 class BPEngine:
@@ -74,6 +104,7 @@ class BPEngine:
                        if precision == "bf16" else None)
         self._bf16_stale = True
         self._canon_graphs = {}  # canonicalise(): eps -> {message buffer at start -> (graph, outputs)}
+        self.status = _lib.DQZ_OK  # of the last run / run_graphed
 
     def _arena(self, n):
         return torch.zeros(max(n, 1), dtype=self.dtype, device=self.layout.device)
@@ -128,6 +159,106 @@ class BPEngine:
     def read_messages_host(self, out_n2e: torch.Tensor) -> None:
         out_n2e.copy_(self.n2e, non_blocking=True)
 
+    def sweep_host(self, packed: torch.Tensor, n2e_host: torch.Tensor, e2n_host: torch.Tensor,
+                   out_n2e: torch.Tensor, chunks: int = 8) -> None:
+        """load_tensors_host + load_messages_host + sweep + read_messages_host
+        with the copies overlapped with the kernels: the messages go first,
+        then the node tensors in ``chunks`` ranges of nodes, on an upload
+        stream; each range is packed and updated as soon as it has arrived, and
+        its new node->edge messages go back to ``out_n2e`` on a download stream
+        while later ranges are still arriving. Same result as the unpipelined
+        sequence, bit for bit. Synchronous sweeps of uniform degree-3 graphs
+        (one node level; FP64, FP32 or the tcgen05 BF16 form); other engines
+        run the plain sequence. Host tensors must be pinned."""
+        L, topo = self.layout, self.topo
+        if (chunks <= 1 or len(topo.levels) != 1 or not L.uniform_k3_chi()
+                or (self.T_bf16 is not None and self.bf16_kernel != "tcgen05")):
+            self.load_tensors_host(packed)
+            self.load_messages_host(n2e_host, e2n_host)
+            self.sweep()
+            self.read_messages_host(out_n2e)
+            return
+        cur = torch.cuda.current_stream()
+        if getattr(self, "_xfer", None) is None:
+            self._xfer = (torch.cuda.Stream(device=L.device), torch.cuda.Stream(device=L.device))
+            self._chunk_lists = {}
+        up, down = self._xfer
+        n = L.n_nodes
+        plan = self._chunk_lists.get(chunks)
+        if plan is None:
+            bounds = sorted(set(round(i * n / chunks) for i in range(chunks + 1)))
+            t_off = [int(x) for x in L.node_off] + [L.tensor_elems]
+            h_off = [int(x) for x in L.node_half] + [L.n_halves]
+            m_off = [int(L.half_msg_off[h]) for h in h_off[:-1]] + [L.msg_elems]
+            plan = []
+            for lo, hi in zip(bounds[:-1], bounds[1:]):
+                ids = (torch.arange(lo, hi, dtype=torch.int32, device=L.device) if self.T_bf16 is not None else
+                       torch.arange(h_off[lo], h_off[hi], dtype=torch.int32, device=L.device))
+                plan.append((lo, hi, t_off[lo], t_off[hi], m_off[lo], m_off[hi], ids))
+            self._chunk_lists[chunks] = plan
+        src_sel, edge_new, _ = topo.device_tables(L.device)
+        n2e_new, e2n_new = self._spare
+        chi = L.uniform_k3_chi()
+        flag = error_flag(L.device)
+        stream = _lib.stream_handle()
+
+        def stage(src):
+            key = (src.numel(), src.dtype)
+            buf = self._stage.get(key)
+            if buf is None:
+                buf = self._stage[key] = torch.empty(src.numel(), dtype=src.dtype, device=L.device)
+            return buf
+
+        # uploads: wait for the previous step's kernels, then messages, then every node range
+        up.wait_stream(cur)
+        with torch.cuda.stream(up):
+            msg_dst = []
+            for src, dst in ((n2e_host, self.n2e), (e2n_host, self.e2n)):
+                tgt = dst if src.dtype == dst.dtype else stage(src)
+                tgt.copy_(src, non_blocking=True)
+                msg_dst.append((tgt, dst))
+            ev_msgs = up.record_event()
+            t_dst = self.T if packed.dtype == self.T.dtype else stage(packed)
+            ev_t = []
+            for _, _, a, b, _, _, _ in plan:
+                t_dst[a:b].copy_(packed[a:b], non_blocking=True)
+                ev_t.append(up.record_event())
+        cur.wait_event(ev_msgs)
+        for tgt, dst in msg_dst:
+            if tgt is not dst:
+                dst.copy_(tgt)
+        down.wait_stream(cur)  # out_n2e may still be read by an earlier download
+        for (lo, hi, a, b, ma, mb, ids), ev in zip(plan, ev_t):
+            cur.wait_event(ev)
+            if t_dst is not self.T:
+                self.T[a:b].copy_(t_dst[a:b])
+            if self.T_bf16 is not None:
+                _lib.call("dqz_pack_bf16_umma_nodes", L.gptr, self.T.data_ptr(), self.T_bf16.data_ptr(), lo, hi - lo,
+                          stream)
+                _lib.call(BF16_KERNELS["tcgen05"], L.gptr, self.T_bf16.data_ptr(), self.n2e.data_ptr(),
+                          self.e2n.data_ptr(), n2e_new.data_ptr(), src_sel.data_ptr(), ids.data_ptr(), ids.numel(),
+                          flag.data_ptr(), stream)
+            else:
+                _lib.call("dqz_bp_node_update_k3", L.gptr, chi, 64 if self.T.dtype == torch.complex128 else 32,
+                          self.T.data_ptr(), self.n2e.data_ptr(), self.e2n.data_ptr(), n2e_new.data_ptr(),
+                          src_sel.data_ptr(), ids.data_ptr(), ids.numel(), flag.data_ptr(), stream)
+            down.wait_event(cur.record_event())
+            with torch.cuda.stream(down):
+                out_n2e[ma:mb].copy_(n2e_new[ma:mb], non_blocking=True)
+        if self.T.dtype == torch.complex64:
+            _lib.call("dqz_bp_edge_pass_c64", L.gptr, self.n2e.data_ptr(), n2e_new.data_ptr(), edge_new.data_ptr(),
+                      e2n_new.data_ptr(), stream)
+        else:
+            _lib.call("dqz_bp_edge_pass", L.gptr, self.n2e.data_ptr(), n2e_new.data_ptr(), edge_new.data_ptr(),
+                      e2n_new.data_ptr(), chi, stream)
+        if self.T_bf16 is not None:
+            self._bf16_stale = False
+        cur.wait_stream(up)
+        cur.wait_stream(down)
+        self._spare = (self.n2e, self.e2n)
+        self._prev = (self.n2e, self.e2n)
+        self.n2e, self.e2n = n2e_new, e2n_new
+
     # ------------------------------------------------------------ compute
     def sweep(self, mid_event=None) -> None:
         """One BP sweep; the previous message set is kept for ``distance``.
@@ -153,6 +284,15 @@ class BPEngine:
         if int(error_flag(self.layout.device).item()):
             raise RuntimeError("a BP kernel met a node outside its supported shape")
 
+    def check_finite(self) -> None:
+        """Raises NonFiniteError when a node tensor or message holds NaN / Inf
+        (a host-visible check of the loaded state; synchronises)."""
+        for name, t in (("node tensors", self.T), ("node->edge messages", self.n2e),
+                        ("edge->node messages", self.e2n)):
+            bad = _lib.count_nonfinite(t)
+            if bad:
+                raise _lib.NonFiniteError(f"{name}: {bad} non-finite values")
+
     def _c128(self, x: torch.Tensor) -> torch.Tensor:
         return x if x.dtype == torch.complex128 else x.to(torch.complex128)
 
@@ -170,12 +310,16 @@ class BPEngine:
         return out
 
     def run(self, tol: float, max_sweeps: int = 1000, check_every: int = 1) -> int:
-        """Sweeps until distance() <= tol (read back every ``check_every`` sweeps)."""
-        for it in range(1, max_sweeps + 1):
-            self.sweep()
-            if it % check_every == 0 and float(self.distance()) <= tol:
-                return it
-        return max_sweeps
+        """Sweeps until distance() <= tol (read back every ``check_every``
+        sweeps); returns the sweeps done and sets ``status`` (DQZ_OK or
+        DQZ_ERR_NOT_CONVERGED). Raises NonFiniteError on a NaN / Inf distance."""
+
+        def step():
+            for _ in range(check_every):
+                self.sweep()
+
+        done, self.status = converge(step, self.distance, tol, max_sweeps, check_every)
+        return done
 
     def run_graphed(self, tol: float, max_sweeps: int = 1000, block: int = 8) -> int:
         """``run`` with every block of ``block`` sweeps and the distance that
@@ -189,20 +333,21 @@ class BPEngine:
         # happen before capture
         self.sweep()
         self.sweep()
-        done = 2
-        if float(self.distance()) <= tol or done >= max_sweeps:
-            return done
+        d = float(self.distance())
+        if not math.isfinite(d):
+            raise _lib.NonFiniteError(f"BP sweep 2: message distance {d}")
+        self.status = _lib.DQZ_OK
+        if d <= tol or max_sweeps <= 2:
+            if d > tol:
+                self.status = _lib.DQZ_ERR_NOT_CONVERGED
+            return 2
         graph = torch.cuda.CUDAGraph()
         with torch.cuda.graph(graph):
             for _ in range(block):
                 self.sweep()
             dist = self.distance()
         self._graph = graph  # keep the graph (and its memory pool) alive with the engine
-        while done < max_sweeps:
-            graph.replay()
-            done += block
-            if float(dist) <= tol:
-                break
+        done, self.status = converge(graph.replay, lambda: dist, tol, max_sweeps, block, first=2)
         return done
 
     def _rotate(self) -> None:

@@ -138,6 +138,10 @@ size_t dqz_bf16_umma_elems_per_node(void);
 /* complex64 node tensors (node_off layout) -> the BF16 core layouts above. */
 int dqz_pack_bf16_umma(const dqz_graph_t *g, const void *tensors_c64, void *tensors_bf16,
                        cudaStream_t stream);
+/* The same for nodes first .. first + count - 1 only (a pipelined load packs
+ * each chunk of nodes as soon as its tensors have arrived). */
+int dqz_pack_bf16_umma_nodes(const dqz_graph_t *g, const void *tensors_c64, void *tensors_bf16,
+                             int32_t first, int32_t count, cudaStream_t stream);
 
 /* Edge pass on complex64 messages (see dqz_bp_edge_pass). */
 int dqz_bp_edge_pass_c64(const dqz_graph_t *g, const void *n2e_old, const void *n2e_new,
@@ -163,6 +167,13 @@ int dqz_reduce_sum(const double *partial, int32_t n, double scale, double *out, 
  * partial: n doubles of scratch. */
 int dqz_segment_distance(const void *a, const void *b, const int64_t *seg_off, int32_t n,
                          double *partial, double *out, cudaStream_t stream);
+
+/* *count += number of non-finite (NaN or +-Inf) words among the n real words
+ * at data (elem_bytes 8: doubles, 4: floats; a complex array of m entries is
+ * 2m words). The caller zeroes *count. The reference has no such check: its
+ * arithmetic carries NaN through silently; this backs the DQZ_ERR_NONFINITE
+ * status of the host-side loops. */
+int dqz_count_nonfinite(const void *data, int64_t n, int32_t elem_bytes, int32_t *count, cudaStream_t stream);
 
 /* Copies n segments: dst[dst_off[i] .. + count[i]) = src[src_off[i] .. + count[i]),
  * offsets and counts in elements of elem_bytes (8 or 16). Used to move node
@@ -295,7 +306,10 @@ size_t dqz_simple_update_scratch_bytes(int32_t n, int32_t max_rows, int32_t max_
  *    that fit run one after another inside the launch.
  *  - The first call on each device looks up the array's device address
  *    (cudaGetSymbolAddress with that device current); make that first call
- *    before any stream capture.
+ *    before any stream capture. The address is kept for the life of the
+ *    process: calls after a cudaDeviceReset of that device are not supported.
+ *  - The DQZ_TUNE_SU_GRID knob applies as for dqz_simple_update, capped at
+ *    the number of job slices that fit in the array.
  *  - Every call uses the same array and it keeps whatever the last call left
  *    there (the kernel writes every scratch word before reading it). Calls
  *    whose kernels overlap on the GPU -- on different streams, or from

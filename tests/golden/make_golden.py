@@ -16,7 +16,7 @@ the stand-in hands out is an ndarray subclass whose in-place operators
 return new arrays (and whose ``x.at[i].set(v)`` returns an updated copy, as
 in JAX). The module is the reference's source as it is.
 
-Usage: python tests/golden/make_golden.py [path to the reference checkout]
+Usage: python tests/golden/make_golden.py <path to the reference checkout>
 """
 
 import importlib.util
@@ -555,4 +555,6 @@ def graph_ops(D, graph, out, put, tensors, lambdas, rng):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py <path to a checkout of LuchnikovI/dequantizer>")
+    main(sys.argv[1])

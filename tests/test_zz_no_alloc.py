@@ -95,7 +95,11 @@ def _run(entry, L, T, lam, jobs, flat, ranks, rows, cols, max_chi):
     return err, ent
 
 
-def test_noalloc_matches_allocating_entry_point_twice():
+@pytest.mark.parametrize("stride_rows", [None, 12000, 30000])
+def test_noalloc_matches_allocating_entry_point_twice(stride_rows):
+    """stride_rows: a larger row bound than the jobs need (the kernels use it
+    only as the stride of their scratch slices), so that 2 or 1 job slices
+    fit in the library's array and the jobs of one call share them in turn."""
     g, L_a, T_a, lam_a, max_chi, rng = _state(3)
     _, L_b, T_b, lam_b, _, _ = _state(3)
     rng_a, rng_b = np.random.default_rng(99), np.random.default_rng(99)
@@ -104,6 +108,11 @@ def test_noalloc_matches_allocating_entry_point_twice():
         jobs, flat, ranks, rows, cols = _batch(L_a, used_a, rng_a, max_chi)
         jobs_b, flat_b, ranks_b, rows_b, cols_b = _batch(L_b, used_b, rng_b, max_chi)
         assert jobs == jobs_b and rows == rows_b and cols == cols_b
+        if stride_rows is not None:
+            cols = 16
+            rows = rows_b = stride_rows
+            slots = (32 << 20) // (64 * rows * cols)
+            assert slots in (1, 2) and len(jobs) > slots
         used_a |= set(jobs)
         used_b |= set(jobs)
         err_a, ent_a = _run("dqz_simple_update", L_a, T_a, lam_a, jobs, flat, ranks, rows, cols, max_chi)
