@@ -3,6 +3,8 @@
 //  * apply_half_gates  -- tensor_ops.py:221-262 (untruncated apply2)
 //  * simple_update     -- tensor_ops.py:265-389 (+ tensor_graph.py:294-375),
 //                         one CTA per edge of a node-disjoint batch.
+#include <cooperative_groups.h>
+
 #include "linalg.cuh"
 
 using namespace dqz;
@@ -205,6 +207,65 @@ __device__ void su_write(const SUSide &S, const cd *X, int rank, cd *T, double e
   }
 }
 
+// Jobs whose A matrix has fewer rows on both sides (bonds below 16 between
+// degree-3 nodes) stay on the global-scratch kernel, which runs several jobs
+// per SM; the on-chip form takes the larger ones that fit.
+constexpr int SUF_MIN_ROWS = 256;
+
+// Dimensions of one side of a job in the shared-memory form (below):
+//   B = lambda-weighted node tensor, rows b (the other bonds), columns (a, i)
+//       (updated bond, physical index): MB x KB;
+//   S = R_B with the half gate applied, rows (c, o), columns (a, rho): MS x KS;
+//   muB / muS = min(rows, columns): reflector counts, rows of R.
+struct SufDims {
+  int MB, KB, muB, MS, KS, muS;
+};
+
+__device__ __forceinline__ void suf_dims(const SUSide &S, int r, SufDims &D) {
+  const int ce = S.dims[S.slot];
+  D.MB = S.M / S.d;
+  D.KB = ce * S.d;
+  D.muB = D.MB < D.KB ? D.MB : D.KB;
+  D.MS = D.muB * S.d;
+  D.KS = ce * r;
+  D.muS = D.MS < D.KS ? D.MS : D.KS;
+}
+
+__host__ __device__ __forceinline__ long long suf_even(long long x) { return (x + 1) & ~1ll; }
+
+// Largest kept rank of a job: max_rank when it cuts below K = KS, else K.
+__host__ __device__ __forceinline__ int suf_rank_bound(int K, int max_rank) {
+  return (max_rank > 0 && max_rank < K) ? max_rank : K;
+}
+
+// Size of the combined core | W region: the core SVD needs 2 K^2; later the
+// same space holds V^H V (muB^2) and then V^H Z (muB x d*rank).
+__device__ __forceinline__ long long suf_cw(const SufDims &D, int d, int rk) {
+  const long long K = D.KS;
+  long long cw = 2 * K * K;
+  const long long g = (long long)D.muB * (D.muB > d * rk ? D.muB : d * rk);
+  return suf_even(cw > g ? cw : g);
+}
+
+// Complex entries of one side's shared-memory layout, in this order:
+//   S [MS*KS] | tauS [muS] | B [MB*KB] | tauB [muB] | core, W [cw] | X [MS*rk]
+__device__ __forceinline__ long long suf_need(const SufDims &D, int d, int rk) {
+  return suf_even((long long)D.MS * D.KS) + suf_even(D.muS) + suf_even((long long)D.MB * D.KB) + suf_even(D.muB) +
+         suf_cw(D, d, rk) + suf_even((long long)D.MS * rk);
+}
+
+// Whether a job runs in the shared-memory form with `cap` complex entries
+// per CTA. Both CTAs of a cluster, and the fallback kernel, decide alike.
+__device__ __forceinline__ bool suf_fits(const SUSide &U, const SUSide &V, int r, int max_rank, long long cap) {
+  if (cap <= 0 || (U.M < SUF_MIN_ROWS && V.M < SUF_MIN_ROWS)) return false;
+  SufDims du, dv;
+  suf_dims(U, r, du);
+  suf_dims(V, r, dv);
+  if (du.KS > DQZ_MAX_CHI) return false;
+  const int rk = suf_rank_bound(du.KS, max_rank);
+  return suf_need(du, U.d, rk) <= cap && suf_need(dv, V.d, rk) <= cap;
+}
+
 __host__ __device__ inline size_t su_scratch_per_job(int max_rows, int max_cols) {
   return 4 * (size_t)max_rows * max_cols * sizeof(cd);
 }
@@ -212,7 +273,7 @@ __host__ __device__ inline size_t su_scratch_per_job(int max_rows, int max_cols)
 __global__ void __launch_bounds__(GATE_THREADS) simple_update_kernel(
     dqz_graph_t g, cd *Tall, double *lambdas, const int32_t *edges, const uint8_t *ctrl_first, const cd *halves,
     const int32_t *ranks, int n, double eps, int max_rank, int max_rows, int max_cols, double *err_out,
-    double *ent_out, cd *scratch) {
+    double *ent_out, cd *scratch, long long fused_cap) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double *red = reinterpret_cast<double *>(smem_raw);
   int *flag = reinterpret_cast<int *>(red + 48);
@@ -234,6 +295,7 @@ __global__ void __launch_bounds__(GATE_THREADS) simple_update_kernel(
     su_load_side(g, lambdas, hu, U);
     su_load_side(g, lambdas, hv, V);
     const int r = ranks[j];
+    if (suf_fits(U, V, r, max_rank, fused_cap)) continue;  // done by the shared-memory form
     const int ce = U.dims[U.slot];
     const int K = ce * r;
     cd *Au = scratch + (size_t)blockIdx.x * (su_scratch_per_job(max_rows, max_cols) / sizeof(cd));
@@ -333,6 +395,284 @@ size_t su_smem_bytes(int max_cols) {
          2 * (size_t)max_cols * sizeof(int);
 }
 
+// ------------------------------------------------ simple update, on chip
+// The same job (tensor_ops.py:265-389) with every matrix in shared memory, for
+// jobs that fit (bonds up to 16 between degree-3 nodes, rank-2 gates). One
+// cluster of two CTAs per job: CTA 0 works on the controlling side, CTA 1 on
+// the controlled side, each on its own SM.
+//  * The side's matrix A[(b, o), (a, rho)] = sum_i B[b, (a, i)] h[rho][o][i]
+//    (b: the other bonds, o / i: physical out / in, a: the updated bond,
+//    rho: gate rank, B = lambda-weighted node tensor) factors in two steps:
+//    B = Q_B R_B (Householder, MB x KB), then S = R_B h = Q_S R_S (Householder,
+//    MS x KS with MS = min(MB, KB) d), so A = (Q_B x I_o) Q_S R_S: R_A = R_S,
+//    the factor the core needs (LAPACK's R up to the signs of its rows, a
+//    gauge). B is half the size of A, and S is small.
+//  * The two CTAs swap R_S through distributed shared memory, build the same
+//    core R_u diag(lambda) R_v^T and run the same SVD (bit-identical in both).
+//  * Gamma = (Q_B x I_o) Q_S [U; 0] / lambda: Q_S by its reflectors, Q_B in
+//    compact-WY form I - V T V^H (LAPACK zlarft), the output rows computed
+//    straight into the node tensor in HBM. No global scratch.
+constexpr int SUF_THREADS = 512;
+constexpr size_t SUF_SMEM_MAX = 220 * 1024;  // dynamic shared memory per CTA (plus ~2.3 KB static)
+
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(SUF_THREADS, 1)
+    simple_update_onchip_kernel(dqz_graph_t g, cd *Tall, double *lambdas, const int32_t *edges,
+                                const uint8_t *ctrl_first, const cd *halves, const int32_t *ranks, int n, double eps,
+                                int max_rank, double *err_out, double *ent_out, long long cap) {
+  namespace cg = cooperative_groups;
+  cg::cluster_group cluster = cg::this_cluster();
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cd *sm = reinterpret_cast<cd *>(smem_raw);
+  __shared__ double red[48];
+  __shared__ int flag[4];
+  __shared__ double sv[DQZ_MAX_CHI], lam_sh[DQZ_MAX_CHI], lam_in[DQZ_MAX_CHI];
+  __shared__ int perm[DQZ_MAX_CHI], acc[DQZ_MAX_CHI];
+  const int side = (int)cluster.block_rank();  // 0: controlling node, 1: controlled node
+  const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
+
+  for (int j = (int)(blockIdx.x >> 1); j < n; j += (int)(gridDim.x >> 1)) {
+    const int e = edges[j];
+    const bool first = ctrl_first[j] != 0;
+    const int hu = g.edge_half[2 * e + (first ? 0 : 1)];
+    const int hv = g.edge_half[2 * e + (first ? 1 : 0)];
+    SUSide U, V;
+    su_load_side(g, lambdas, hu, U);
+    su_load_side(g, lambdas, hv, V);
+    const int r = ranks[j];
+    if (!suf_fits(U, V, r, max_rank, cap)) continue;  // left to the global-scratch kernel; same decision in both CTAs
+    const SUSide &X = side ? V : U;
+    SufDims D, Du, Dv;
+    suf_dims(U, r, Du);
+    suf_dims(V, r, Dv);
+    D = side ? Dv : Du;
+    const int d = X.d, K = D.KS;
+    cd *Sm = sm;
+    cd *tauS = Sm + suf_even((long long)D.MS * D.KS);
+    cd *Bm = tauS + suf_even(D.muS);
+    cd *tauB = Bm + suf_even((long long)D.MB * D.KB);
+    cd *core = tauB + suf_even(D.muB);
+    cd *W = core + (long long)K * K;
+    cd *Xm = core + suf_cw(D, d, suf_rank_bound(K, max_rank));
+    const cd *H = halves + (long long)j * 2 * HALF_STRIDE + side * HALF_STRIDE;
+    cd *T = Tall + g.node_off[X.node];
+
+    // ---- B[b, (a, i)] = wt(b) T[.., a, .., i], column-major (ld MB)
+    {
+      const int ce = X.dims[X.slot];
+      const long long total = (long long)D.MB * D.KB;
+      for (long long idx = tid; idx < total; idx += nt) {
+        const int i = (int)(idx % d);
+        const long long t = idx / d;
+        const int a = (int)(t % ce);
+        const int b = (int)(t / ce);
+        long long rem = b, off = 0;
+        double wt = 1.0;
+        for (int f = X.k - 1; f >= 0; --f) {
+          if (f == X.slot) continue;
+          const int af = (int)(rem % X.dims[f]);
+          rem /= X.dims[f];
+          off += af * X.stride[f];
+          wt *= X.lam[f][af];
+        }
+        Bm[b + (long long)(a * d + i) * D.MB] = cscale(T[off + a * X.stride[X.slot] + i], wt);
+      }
+      __syncthreads();
+    }
+    householder_qr(Bm, D.MB, D.KB, tauB, red);
+
+    // ---- S[(c, o), (a, rho)] = sum_i R_B[c, (a, i)] h[rho][o][i], normalised (|A|_F = |S|_F)
+    {
+      double n2 = 0.0;
+      const long long total = (long long)D.MS * D.KS;
+      for (long long idx = tid; idx < total; idx += nt) {
+        const int row = (int)(idx % D.MS), col = (int)(idx / D.MS);
+        const int c = row / d, o = row % d, a = col / r, rho = col % r;
+        cd v = czero();
+        for (int i = 0; i < d; ++i) {
+          const int cb = a * d + i;
+          if (cb >= c) cfma(v, Bm[c + (long long)cb * D.MB], H[(rho * d + o) * d + i]);
+        }
+        Sm[idx] = v;
+        n2 += cabs2(v);
+      }
+      n2 = block_sum(n2, red);
+      const double inv = 1.0 / sqrt(n2);
+      for (long long idx = tid; idx < total; idx += nt) Sm[idx] = cscale(Sm[idx], inv);
+      __syncthreads();
+    }
+    householder_qr(Sm, D.MS, D.KS, tauS, red);
+
+    // ---- swap R_S: the partner's R (muS x K, upper trapezoidal) into W, then the core
+    cluster.sync();
+    const SufDims &Dp = side ? Du : Dv;
+    {
+      const cd *Sp = cluster.map_shared_rank(Sm, side ^ 1);
+      for (int idx = tid; idx < Dp.muS * K; idx += nt) {
+        const int i = idx % Dp.muS, c = idx / Dp.muS;
+        W[idx] = c >= i ? Sp[i + (long long)c * Dp.MS] : czero();
+      }
+    }
+    // lambda of the updated bond, read before CTA 0 can overwrite it at the end of the job
+    for (int c = tid; c < X.dims[X.slot]; c += nt) lam_in[c] = lambdas[g.edge_lam_off[e] + c];
+    cluster.sync();  // both copies done: S may be overwritten from here on
+    const int mu = Du.muS, mv = Dv.muS;
+    const cd *Ru = side ? W : Sm;
+    const cd *Rv = side ? Sm : W;
+    const int ldu_r = side ? mu : Du.MS, ldv_r = side ? Dv.MS : mv;
+    const int kk = mu < mv ? mu : mv;
+    const bool tall = mu >= mv;
+    const int zr = tall ? mu : mv;
+    for (int idx = tid; idx < mu * mv; idx += nt) {  // core = R_u diag(lambda_e x 1_r) R_v^T (Z of the old form)
+      const int i = idx % mu, jj = idx / mu;
+      cd v = czero();
+      for (int c = (i > jj ? i : jj); c < K; ++c)
+        cfma(v, cscale(Ru[i + (long long)c * ldu_r], lam_in[c / r]), Rv[jj + (long long)c * ldv_r]);
+      if (tall)
+        core[jj * mu + i] = v;
+      else
+        core[i * mv + jj] = cconj(v);
+    }
+    __syncthreads();
+    hestenes(core, zr, zr, kk, W, kk, sv, flag, red);
+    sort_desc(sv, kk, perm);
+    const int rank = (max_rank > 0 && max_rank < kk) ? max_rank : kk;
+    for (int idx = tid; idx < zr * kk; idx += nt) {
+      const int c = idx / zr;
+      const double sc = sv[c];
+      core[idx] = sc > 1e-300 ? cscale(core[idx], 1.0 / sc) : czero();
+    }
+    for (int p = tid; p < kk; p += nt) {
+      const int c = perm[p];
+      acc[c] = (sv[c] > 1e-300 || p >= rank) ? 1 : 0;
+    }
+    __syncthreads();
+    complete_orthonormal(core, zr, zr, kk, acc);
+    const cd *Ub = tall ? core : W;
+    const cd *Vb = tall ? W : core;
+    const int ldu = tall ? mu : kk, ldv = tall ? kk : mv;
+    {
+      double n2 = 0.0;
+      for (int c = tid; c < kk; c += nt) {
+        const double l = safe_truncate(sv[perm[c]], eps);
+        lam_sh[c] = l;
+        n2 += l * l;
+      }
+      n2 = block_sum(n2, red);
+      if (side == 0 && tid == 0) {
+        double ent = 0.0, er = 0.0;
+        for (int c = 0; c < kk; ++c) {
+          const double p = lam_sh[c] * lam_sh[c] / n2;
+          if (p > 0.0) ent -= p * log(p);
+          if (c >= rank) er += p;
+        }
+        err_out[j] = sqrt(er);
+        ent_out[j] = ent;
+      }
+    }
+    // X = [U[:, perm[:rank]]; 0] (controlling side) or [conj(V)[:, perm[:rank]]; 0], MS x rank
+    {
+      const int myu = side ? mv : mu;
+      for (int idx = tid; idx < D.MS * rank; idx += nt) {
+        const int i = idx % D.MS, c = idx / D.MS;
+        cd v = czero();
+        if (i < myu) v = side ? cconj(Vb[(long long)perm[c] * ldv + i]) : Ub[(long long)perm[c] * ldu + i];
+        Xm[idx] = v;
+      }
+      __syncthreads();
+    }
+    apply_q(Sm, D.MS, D.muS, tauS, Xm, D.MS, rank);  // X <- Q_S X (its trailing barrier orders the reads below)
+
+    // ---- compact WY of Q_B = H_0 .. H_{k-1} = I - V T V^H, k = muB
+    const int k = D.muB, p = d * rank;
+    cd *G = core;  // V^H V, then V^H Z, then T V^H Z (k x max(k, p)), column-major ld k
+    cd *Tw = Sm;   // T, k x k upper triangular, ld k (S is no longer needed)
+    auto vb = [&](int row, int c) -> cd {  // V[row, c], row >= c
+      return row == c ? mk(1.0, 0.0) : Bm[row + (long long)c * D.MB];
+    };
+    for (int pr = warp; pr < k * k; pr += nw) {  // G[i, jj] for i < jj, one warp each
+      const int i = pr % k, jj = pr / k;
+      if (i >= jj) continue;
+      cd v = czero();
+      for (int row = jj + lane; row < D.MB; row += 32) cfmac(v, Bm[row + (long long)i * D.MB], vb(row, jj));
+      v = warp_csum(v);
+      if (lane == 0) G[i + (long long)jj * k] = v;
+    }
+    __syncthreads();
+    if (warp == 0) {  // T[:j, j] = T[:j, :j] (-tau_j G[:j, j]), T[j, j] = tau_j (zlarft, forward, columnwise)
+      for (int jj = 0; jj < k; ++jj) {
+        const cd tj = tauB[jj];
+        for (int i0 = 0; i0 < jj; i0 += 32) {
+          const int i = i0 + lane;
+          cd v = czero();
+          if (i < jj)
+            for (int l = i; l < jj; ++l) cfma(v, Tw[i + (long long)l * k], G[l + (long long)jj * k]);
+          __syncwarp();
+          if (i < jj) Tw[i + (long long)jj * k] = cmul(mk(-tj.x, -tj.y), v);
+          __syncwarp();
+        }
+        if (lane == 0) Tw[jj + (long long)jj * k] = tj;
+        for (int i = jj + 1 + lane; i < k; i += 32) Tw[i + (long long)jj * k] = czero();
+        __syncwarp();
+      }
+    }
+    __syncthreads();
+    // V^H Z (k x p): Z[row, q = col * d + o] = X[row * d + o, col] for row < k
+    for (int idx = tid; idx < k * p; idx += nt) {
+      const int c = idx % k, q = idx / k;
+      const int col = q / d, o = q % d;
+      cd v = czero();
+      for (int row = c; row < k; ++row) cfmac(v, vb(row, c), Xm[(row * d + o) + (long long)col * D.MS]);
+      G[idx] = v;
+    }
+    __syncthreads();
+    for (int q = tid; q < p; q += nt) {  // in place: G[:, q] <- T G[:, q] (row i reads rows >= i)
+      cd *gq = G + (long long)q * k;
+      for (int i = 0; i < k; ++i) {
+        cd v = czero();
+        for (int l = i; l < k; ++l) cfma(v, Tw[i + (long long)l * k], gq[l]);
+        gq[i] = v;
+      }
+    }
+    __syncthreads();
+    // ---- Gamma[b, .., col, .., o] = ((Q_B Z)[b, q]) * prod safe_inv(lambda), bond `rank`
+    {
+      long long nst[DQZ_MAX_DEGREE];
+      long long st = d;
+      for (int f = X.k - 1; f >= 0; --f) {
+        nst[f] = st;
+        st *= (f == X.slot) ? rank : X.dims[f];
+      }
+      const long long total = (long long)D.MB * p;
+      for (long long idx = tid; idx < total; idx += nt) {
+        const int q = (int)(idx % p);
+        const int b = (int)(idx / p);
+        const int col = q / d, o = q % d;
+        cd v = b < k ? Xm[(b * d + o) + (long long)col * D.MS] : czero();
+        const cd *gq = G + (long long)q * k;
+        const int cmax = b < k ? b : k - 1;
+        for (int c = 0; c <= cmax; ++c) v = csub(v, cmul(vb(b, c), gq[c]));
+        long long rem = b, off = o + (long long)col * nst[X.slot];
+        double wt = 1.0;
+        for (int f = X.k - 1; f >= 0; --f) {
+          if (f == X.slot) continue;
+          const int af = (int)(rem % X.dims[f]);
+          rem /= X.dims[f];
+          off += af * nst[f];
+          wt *= safe_inverse(X.lam[f][af], eps);
+        }
+        T[off] = cscale(v, wt);
+      }
+    }
+    if (side == 0) {
+      double *lam_out = lambdas + g.edge_lam_off[e];
+      for (int c = tid; c < rank; c += nt) lam_out[c] = lam_sh[c];
+      if (tid == 0) g.edge_chi[e] = rank;
+    }
+    // the next job reads lambdas (this edge's, written by CTA 0) and edge_chi
+    cluster.sync();
+  }
+}
+
 constexpr int SU_GRID_MAX = 148 * 4;
 
 }  // namespace
@@ -373,13 +713,29 @@ extern "C" int dqz_simple_update(const dqz_graph_t *g, void *tensors, double *la
   if (n == 0) return DQZ_OK;
   const size_t smem = su_smem_bytes(max_cols);
   if (smem > SMEM_LIMIT) return DQZ_ERR_UNSUPPORTED;
+  // jobs of A matrices with 256 rows or more (bond 16 and up between degree-3
+  // nodes) go to the on-chip form where they fit; the global-scratch kernel
+  // below then takes only the others
+  long long fused_cap = 0;
+  if (max_rows >= SUF_MIN_ROWS) {
+    DQZ_SMEM_ATTR_ONCE(simple_update_onchip_kernel, SUF_SMEM_MAX);
+    fused_cap = (long long)(SUF_SMEM_MAX / sizeof(cd));
+    int dev = 0, sms = 148;
+    if (cudaGetDevice(&dev) != cudaSuccess) return DQZ_ERR_CUDA;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int pairs = n < sms / 2 ? n : sms / 2;  // one CTA per SM, two per cluster
+    simple_update_onchip_kernel<<<2 * pairs, SUF_THREADS, SUF_SMEM_MAX, stream>>>(
+        *g, (cd *)tensors, lambdas, edges, ctrl_is_first, (const cd *)halves, ranks, n, eps, max_rank, err, entropy,
+        fused_cap);
+    DQZ_CHECK_LAUNCH();
+  }
   DQZ_SMEM_ATTR_ONCE(simple_update_kernel, SMEM_LIMIT);
   int grid = n < SU_GRID_MAX ? n : SU_GRID_MAX;
   const int tuned = dqz_get_tuning(DQZ_TUNE_SU_GRID);  // never above the scratch sizing (SU_GRID_MAX)
   if (tuned > 0 && tuned < grid) grid = tuned;
   simple_update_kernel<<<grid, GATE_THREADS, smem, stream>>>(*g, (cd *)tensors, lambdas, edges, ctrl_is_first,
                                                              (const cd *)halves, ranks, n, eps, max_rank, max_rows,
-                                                             max_cols, err, entropy, (cd *)scratch);
+                                                             max_cols, err, entropy, (cd *)scratch, fused_cap);
   DQZ_CHECK_LAUNCH();
   return DQZ_OK;
 }
@@ -443,7 +799,7 @@ extern "C" int dqz_simple_update_noalloc(const dqz_graph_t *g, void *tensors, do
   DQZ_SMEM_ATTR_ONCE(simple_update_kernel, SMEM_LIMIT);
   simple_update_kernel<<<grid, GATE_THREADS, smem, stream>>>(*g, (cd *)tensors, lambdas, edges, ctrl_is_first,
                                                              (const cd *)halves, ranks, n, eps, max_rank, max_rows,
-                                                             max_cols, err, entropy, (cd *)scratch);
+                                                             max_cols, err, entropy, (cd *)scratch, 0ll);
   DQZ_CHECK_LAUNCH();
   return DQZ_OK;
 }
