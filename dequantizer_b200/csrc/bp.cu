@@ -29,6 +29,64 @@ __device__ __forceinline__ const cd *incoming_msg(const dqz_graph_t &g, int hf, 
   return (sel == DQZ_SRC_N2E_NEW ? n2e_new : n2e_old) + g.half_msg_off[tw];
 }
 
+// n2e_new[h] for one half-edge h by the whole CTA (out: ce x ce, bufA / bufB:
+// two slices, trace_sh: one shared complex). Ends with a barrier.
+__device__ __forceinline__ void node_update_half(const dqz_graph_t &g, const cd *__restrict__ T, const cd *n2e_old,
+                                                 const cd *e2n_old, cd *n2e_new, const uint8_t *__restrict__ src_sel,
+                                                 int h, cd *out, cd *bufA, cd *bufB, cd &trace_sh) {
+  const int v = g.half_node[h];
+  NodeShape s;
+  load_shape(g, v, s);
+  const int e = h - s.half0;
+  const int ce = s.dims[e];
+  const cd *Tv = T + g.node_off[v];
+  const long long Re = s.stride[e];
+  const long long P = s.size / ce;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+
+  for (int a = 0; a < ce; ++a) {
+    for (long long x = threadIdx.x; x < P; x += blockDim.x) {
+      long long l = x / Re, r = x - l * Re;
+      bufA[x] = Tv[(l * ce + a) * Re + r];
+    }
+    __syncthreads();
+    cd *cur = bufA, *nxt = bufB;
+    long long Lj = 1;
+    for (int f = 0; f < s.k; ++f) {
+      if (f == e) continue;
+      const int q = s.dims[f];
+      const long long R = P / Lj / q;
+      const cd *m = incoming_msg(g, s.half0 + f, n2e_old, e2n_old, n2e_new, src_sel);
+      mode_product<false>(cur, nxt, Lj, q, q, R, m, q, 1);
+      __syncthreads();
+      cd *t = cur;
+      cur = nxt;
+      nxt = t;
+      Lj *= q;
+    }
+    for (int ap = warp; ap < ce; ap += nw) {
+      cd acc = czero();
+      for (long long x = lane; x < P; x += 32) {
+        long long l = x / Re, r = x - l * Re;
+        cfmac(acc, Tv[(l * ce + ap) * Re + r], cur[x]);
+      }
+      acc = warp_csum(acc);
+      if (lane == 0) out[ap * ce + a] = acc;
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    cd tr = czero();
+    for (int i = 0; i < ce; ++i) tr = cadd(tr, out[i * ce + i]);
+    trace_sh = tr;
+  }
+  __syncthreads();
+  const cd tr = trace_sh;
+  cd *dst = n2e_new + g.half_msg_off[h];
+  for (int i = threadIdx.x; i < ce * ce; i += blockDim.x) dst[i] = cdiv(out[i], tr);
+  __syncthreads();
+}
+
 __global__ void __launch_bounds__(BP_THREADS) bp_node_generic(dqz_graph_t g, const cd *__restrict__ T,
                                                               const cd *n2e_old, const cd *e2n_old, cd *n2e_new,
                                                               const uint8_t *__restrict__ src_sel,
@@ -44,60 +102,74 @@ __global__ void __launch_bounds__(BP_THREADS) bp_node_generic(dqz_graph_t g, con
   }
   bufB = bufA + max_slice;
   __shared__ cd trace_sh;
+  for (int item = blockIdx.x; item < n_halves; item += gridDim.x)
+    node_update_half(g, T, n2e_old, e2n_old, n2e_new, src_sel, halves[item], out, bufA, bufB, trace_sh);
+}
 
-  for (int item = blockIdx.x; item < n_halves; item += gridDim.x) {
-    const int h = halves[item];
-    const int v = g.half_node[h];
-    NodeShape s;
-    load_shape(g, v, s);
-    const int e = h - s.half0;
-    const int ce = s.dims[e];
-    const cd *Tv = T + g.node_off[v];
-    const long long Re = s.stride[e];
-    const long long P = s.size / ce;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-
-    for (int a = 0; a < ce; ++a) {
-      for (long long x = threadIdx.x; x < P; x += blockDim.x) {
-        long long l = x / Re, r = x - l * Re;
-        bufA[x] = Tv[(l * ce + a) * Re + r];
-      }
-      __syncthreads();
-      cd *cur = bufA, *nxt = bufB;
-      long long Lj = 1;
-      for (int f = 0; f < s.k; ++f) {
-        if (f == e) continue;
-        const int q = s.dims[f];
-        const long long R = P / Lj / q;
-        const cd *m = incoming_msg(g, s.half0 + f, n2e_old, e2n_old, n2e_new, src_sel);
-        mode_product<false>(cur, nxt, Lj, q, q, R, m, q, 1);
-        __syncthreads();
-        cd *t = cur;
-        cur = nxt;
-        nxt = t;
-        Lj *= q;
-      }
-      for (int ap = warp; ap < ce; ap += nw) {
-        cd acc = czero();
-        for (long long x = lane; x < P; x += 32) {
-          long long l = x / Re, r = x - l * Re;
-          cfmac(acc, Tv[(l * ce + ap) * Re + r], cur[x]);
+// Grid-wide barrier for a cooperative launch: one arrival counter and one
+// generation word (sync[0], sync[1], zero at launch). The last block to arrive
+// resets the counter and advances the generation; the others poll it, at
+// most `limit` times. Returns false in every thread of a block that gave up
+// (it has set *error_flag to 3).
+__device__ __forceinline__ bool grid_barrier(unsigned *sync, unsigned &gen, int *error_flag) {
+  __shared__ int ok_sh;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int ok = 1;
+    __threadfence();
+    const unsigned target = gen + 1;
+    if (atomicAdd(&sync[0], 1u) == gridDim.x - 1) {
+      atomicExch(&sync[0], 0u);
+      __threadfence();
+      atomicExch(&sync[1], target);
+    } else {
+      ok = 0;
+      for (int it = 0; it < (1 << 24); ++it) {
+        if (atomicAdd(&sync[1], 0u) == target) {
+          ok = 1;
+          break;
         }
-        acc = warp_csum(acc);
-        if (lane == 0) out[ap * ce + a] = acc;
+        __nanosleep(32);
       }
-      __syncthreads();
+      if (!ok) atomicExch(error_flag, 3);
     }
-    if (threadIdx.x == 0) {
-      cd tr = czero();
-      for (int i = 0; i < ce; ++i) tr = cadd(tr, out[i * ce + i]);
-      trace_sh = tr;
-    }
-    __syncthreads();
-    const cd tr = trace_sh;
-    cd *dst = n2e_new + g.half_msg_off[h];
-    for (int i = threadIdx.x; i < ce * ce; i += blockDim.x) dst[i] = cdiv(out[i], tr);
-    __syncthreads();
+    __threadfence();
+    ok_sh = ok;
+  }
+  __syncthreads();
+  ++gen;
+  return ok_sh != 0;
+}
+
+// A whole sweep in one cooperative launch: node levels in order (the
+// asynchronous schedule's dependency levels), a grid barrier after each, then
+// the edge pass. Every half-edge is computed exactly as bp_node_generic does.
+__global__ void __launch_bounds__(BP_THREADS) bp_sweep_levels_kernel(
+    dqz_graph_t g, const cd *__restrict__ T, const cd *n2e_old, const cd *e2n_old, cd *n2e_new, cd *e2n_new,
+    const uint8_t *__restrict__ src_sel, const uint8_t *__restrict__ edge_new, const int32_t *__restrict__ halves,
+    const int32_t *__restrict__ level_off, int n_levels, int max_slice, int max_chi, unsigned *sync,
+    int *error_flag) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cd *out = reinterpret_cast<cd *>(smem_raw + 48 * sizeof(double));
+  cd *bufA = out + (long long)max_chi * max_chi;
+  cd *bufB = bufA + max_slice;
+  __shared__ cd trace_sh;
+  unsigned gen = 0;
+  for (int lv = 0; lv < n_levels; ++lv) {
+    for (int item = level_off[lv] + blockIdx.x; item < level_off[lv + 1]; item += gridDim.x)
+      node_update_half(g, T, n2e_old, e2n_old, n2e_new, src_sel, halves[item], out, bufA, bufB, trace_sh);
+    if (!grid_barrier(sync, gen, error_flag)) return;
+  }
+  // edge pass: e2n_new[h] = (edge_new[h] ? n2e_new : n2e_old)[twin(h)], one warp per half-edge
+  const int wpb = blockDim.x >> 5;
+  for (int h = blockIdx.x * wpb + (threadIdx.x >> 5); h < g.n_halves; h += gridDim.x * wpb) {
+    const int e = g.half_edge[h];
+    const int tw = g.half_twin[h];
+    if (e < 0 || tw < 0) continue;
+    const int c = g.edge_chi[e];
+    const cd *src = (edge_new[h] ? n2e_new : n2e_old) + g.half_msg_off[tw];
+    cd *dst = e2n_new + g.half_msg_off[h];
+    warp_copy16(reinterpret_cast<uint4 *>(dst), reinterpret_cast<const uint4 *>(src), c * c);
   }
 }
 
@@ -221,5 +293,45 @@ extern "C" int dqz_reduce_sum(const double *partial, int32_t n, double scale, do
   if (!partial || !out || n <= 0) return DQZ_ERR_ARG;
   reduce_sum_kernel<<<1, 256, 0, stream>>>(partial, n, scale, out);
   DQZ_CHECK_LAUNCH();
+  return DQZ_OK;
+}
+
+extern "C" int dqz_bp_sweep_levels(const dqz_graph_t *g, const void *tensors, const void *n2e_old,
+                                   const void *e2n_old, void *n2e_new, void *e2n_new, const uint8_t *src_sel,
+                                   const uint8_t *edge_new, const int32_t *halves, const int32_t *level_off,
+                                   int32_t n_levels, int32_t max_level, int32_t max_slice, int32_t max_chi,
+                                   uint32_t *sync, int32_t *error_flag, cudaStream_t stream) {
+  if (!g || !tensors || !n2e_old || !e2n_old || !n2e_new || !e2n_new || !src_sel || !edge_new || !halves ||
+      !level_off || !sync || !error_flag || n_levels <= 0 || max_level <= 0 || max_slice <= 0)
+    return DQZ_ERR_ARG;
+  if (max_chi <= 0 || max_chi > DQZ_MAX_CHI) return DQZ_ERR_UNSUPPORTED;
+  const size_t smem = bp_smem_bytes(max_slice, max_chi, false);
+  if (smem > BP_SMEM_LIMIT) return DQZ_ERR_UNSUPPORTED;  // the per-level launches use global scratch then
+  DQZ_SMEM_ATTR_ONCE(bp_sweep_levels_kernel, BP_SMEM_LIMIT);
+  int dev = 0, sms = 148, per_sm = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return DQZ_ERR_CUDA;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bp_sweep_levels_kernel, BP_THREADS, smem) !=
+          cudaSuccess ||
+      per_sm < 1)
+    return DQZ_ERR_UNSUPPORTED;
+  int grid = max_level;  // one CTA per half-edge of the widest level, all co-resident
+  if (grid > sms * per_sm) grid = sms * per_sm;
+  if (cudaMemsetAsync(sync, 0, 2 * sizeof(uint32_t), stream) != cudaSuccess) return DQZ_ERR_CUDA;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(BP_THREADS);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  if (cudaLaunchKernelEx(&cfg, bp_sweep_levels_kernel, *g, (const cd *)tensors, (const cd *)n2e_old,
+                         (const cd *)e2n_old, (cd *)n2e_new, (cd *)e2n_new, src_sel, edge_new, halves, level_off,
+                         (int)n_levels, (int)max_slice, (int)max_chi, (unsigned *)sync, (int *)error_flag) !=
+      cudaSuccess)
+    return DQZ_ERR_CUDA;
   return DQZ_OK;
 }

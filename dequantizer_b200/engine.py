@@ -62,7 +62,7 @@ def converge(step: Callable[[], None], distance: Callable[[], float], tol: float
     return done, _lib.DQZ_ERR_NOT_CONVERGED
 
 
-PRECISIONS ={"fp64": torch.complex128, "fp32": torch.complex64, "bf16": torch.complex64}
+PRECISIONS = {"fp64": torch.complex128, "fp32": torch.complex64, "bf16": torch.complex64}
 
 
 class BPEngine:
@@ -277,6 +277,8 @@ class BPEngine:
         self.n2e, self.e2n = n2e_new, e2n_new
 
     def launches_per_sweep(self) -> int:
+        if len(self.topo.levels) > 1 and self.T.dtype == torch.complex128 and not self.layout.uniform_k3_chi():
+            return 1  # every level and the edge pass in one cooperative launch (dqz_bp_sweep_levels)
         return len(self.topo.levels) + 1
 
     def check(self) -> None:

@@ -136,6 +136,20 @@ class Topology:
             )
         return self._dev
 
+    def device_level_tables(self, device):
+        """The levels as one flat half-edge list with offsets, the widest
+        level's size, and two words of barrier scratch, for the one-launch sweep
+        (dqz_bp_sweep_levels). Sweeps of one topology share the scratch, so
+        they run on one stream at a time."""
+        if getattr(self, "_dev_flat", None) is None:
+            flat = np.concatenate(self.levels).astype(np.int32) if self.levels else np.zeros(0, np.int32)
+            off = np.zeros(len(self.levels) + 1, dtype=np.int32)
+            off[1:] = np.cumsum([len(l) for l in self.levels])
+            self._dev_flat = (torch.from_numpy(flat).to(device), torch.from_numpy(off).to(device),
+                              max((len(l) for l in self.levels), default=0),
+                              torch.zeros(2, dtype=torch.int32, device=device))
+        return self._dev_flat
+
     def device_node_levels(self, device):
         if self._dev_nodes is None:
             self._dev_nodes = [torch.from_numpy(l).to(device) for l in self.node_levels]
@@ -221,6 +235,20 @@ def bp_sweep(layout: GraphLayout, topo: Topology, T, n2e_old, e2n_old, n2e_new, 
                   e2n_new.data_ptr(), chi3, stream)
         return
     max_slice, max_chi = layout.max_slice(), layout.max_chi()
+    if len(topo.levels) > 1:
+        # a schedule of several node levels (the reference's asynchronous sweep):
+        # all levels and the edge pass in one launch when a slice fits on chip
+        flat, off, widest, sync = topo.device_level_tables(layout.device)
+        status = _lib.lib().dqz_bp_sweep_levels(
+            layout.gptr, T.data_ptr(), n2e_old.data_ptr(), e2n_old.data_ptr(), n2e_new.data_ptr(), e2n_new.data_ptr(),
+            src_sel.data_ptr(), edge_new.data_ptr(), flat.data_ptr(), off.data_ptr(), len(topo.levels), widest,
+            max_slice, max_chi, sync.data_ptr(), error_flag(layout.device).data_ptr(), stream)
+        if status == _lib.DQZ_OK:
+            if mid_event is not None:
+                mid_event.record(torch.cuda.current_stream())
+            return
+        if status != _lib.DQZ_ERR_UNSUPPORTED:
+            _lib.check("dqz_bp_sweep_levels", status)
     scratch = None
     nbytes = _lib.lib().dqz_bp_node_scratch_bytes(max(len(l) for l in topo.levels), max_slice, max_chi)
     if nbytes:

@@ -143,6 +143,23 @@ int dqz_pack_bf16_umma(const dqz_graph_t *g, const void *tensors_c64, void *tens
 int dqz_pack_bf16_umma_nodes(const dqz_graph_t *g, const void *tensors_c64, void *tensors_bf16,
                              int32_t first, int32_t count, cudaStream_t stream);
 
+/* A whole sweep (tensor_ops.py:36-76, mappings/belief_propagation.py:24-64) in
+ * one launch: the node levels of a schedule in order, then the edge pass, with
+ * a grid-wide barrier between levels (a cooperative launch; the grid is sized
+ * so that every CTA is resident). halves[level_off[l] .. level_off[l+1]) are
+ * the half-edges of level l; max_level bounds the half-edges of one level,
+ * max_slice the node-tensor slice (node size / bond dimension), max_chi the
+ * bonds. The results equal one dqz_bp_node_update launch per level followed by
+ * dqz_bp_edge_pass, bit for bit. sync: two device words of scratch (zeroed by
+ * the call). A barrier wait that runs out (seconds) sets *error_flag to 3 and
+ * ends the launch. DQZ_ERR_UNSUPPORTED when a slice does not fit in shared
+ * memory (use the per-level launches then). */
+int dqz_bp_sweep_levels(const dqz_graph_t *g, const void *tensors, const void *n2e_old, const void *e2n_old,
+                        void *n2e_new, void *e2n_new, const uint8_t *src_sel, const uint8_t *edge_new,
+                        const int32_t *halves, const int32_t *level_off, int32_t n_levels, int32_t max_level,
+                        int32_t max_slice, int32_t max_chi, uint32_t *sync, int32_t *error_flag,
+                        cudaStream_t stream);
+
 /* Edge pass on complex64 messages (see dqz_bp_edge_pass). */
 int dqz_bp_edge_pass_c64(const dqz_graph_t *g, const void *n2e_old, const void *n2e_new,
                          const uint8_t *edge_new, void *e2n_new, cudaStream_t stream);

@@ -357,3 +357,44 @@ def test_gauge_knobs_leave_results_unchanged_and_tuner_caches(tmp_path):
         assert autotune.tune_gauge(L, T, n2e, tuner=tuner2) == best and tuner2.timed_keys == []
     finally:
         autotune.set_knobs({k: 0 for k in autotune.KNOBS})
+
+
+@pytest.mark.parametrize("case", ["lattice_3x3x3", "eagle_cell"])
+def test_one_launch_sweep_equals_level_launches(case):
+    """dqz_bp_sweep_levels (every node level of the asynchronous DFS schedule
+    and the edge pass in one cooperative launch, grid barriers between levels)
+    gives one dqz_bp_node_update launch per level plus dqz_bp_edge_pass, bit
+    for bit, over several sweeps."""
+    from dequantizer_b200 import _lib
+    from dequantizer_b200.layout import GraphLayout
+
+    g = G.get_nd_lattice([3, 3, 3], 2, 2) if case == "lattice_3x3x3" else G.get_heavy_hex_ibm_eagle_lattice_infinite()
+    if case == "eagle_cell":
+        for e in g.edges.values():
+            e.dimension = 4
+        g.refresh_bond_shapes()
+    tensors = random_tensors(g, 21)
+    msgs = random_messages(g, 22)
+    topo = M.Topology(list(g.get_traversal_iterator(ordering="dfs")), False)
+    assert len(topo.levels) > 3
+    L = GraphLayout(topo.nodes, topo.edges, [e.dimension for e in topo.edges])
+    T = L.pack_tensors([torch.from_numpy(tensors[n.id]).cuda() for n in topo.nodes])
+    n2e = L.pack_messages([torch.from_numpy(msgs[MessageID(nd.id, e.id)]).cuda() for nd, e in topo.half_ids()])
+    e2n = L.pack_messages([torch.from_numpy(msgs[MessageID(e.id, nd.id)]).cuda() for nd, e in topo.half_ids()])
+    src_sel, edge_new, levels = topo.device_tables(T.device)
+    stream = _lib.stream_handle()
+    a = (n2e.clone(), e2n.clone())
+    b = (n2e.clone(), e2n.clone())
+    for _ in range(3):
+        na, ea = torch.zeros_like(n2e), torch.zeros_like(e2n)
+        M.bp_sweep(L, topo, T, a[0], a[1], na, ea)
+        nb, eb = torch.zeros_like(n2e), torch.zeros_like(e2n)
+        for halves in levels:
+            _lib.call("dqz_bp_node_update", L.gptr, T.data_ptr(), b[0].data_ptr(), b[1].data_ptr(), nb.data_ptr(),
+                      src_sel.data_ptr(), halves.data_ptr(), halves.numel(), L.max_slice(), L.max_chi(), None, stream)
+        _lib.call("dqz_bp_edge_pass", L.gptr, b[0].data_ptr(), nb.data_ptr(), edge_new.data_ptr(), eb.data_ptr(),
+                  L.max_chi(), stream)
+        a, b = (na, ea), (nb, eb)
+        torch.cuda.synchronize()
+        assert torch.equal(a[0], b[0]) and torch.equal(a[1], b[1])
+    assert int(M.error_flag(T.device).item()) == 0
