@@ -591,7 +591,8 @@ def run_anneal(args, world, rank, local):
     n_steps = args.trotter_steps
     dt = 20.0 / n_steps
     s_of = [t / (n_steps - 1) for t in range(n_steps)]
-    ba = BatchedAnnealer(energies, max_chi=args.chi, accuracy=1e-5, max_belief_propagation_iterations=100)
+    ba = BatchedAnnealer(energies, max_chi=args.chi, accuracy=1e-5, max_belief_propagation_iterations=100,
+                         precision=args.anneal_precision)
     torch.cuda.synchronize()
     t = 0
     for _ in range(args.warmup):
@@ -600,7 +601,7 @@ def run_anneal(args, world, rank, local):
         t += 1
     torch.cuda.synchronize()
     barrier(world)
-    sw0 = len(ba.bp_iterations)
+    sw0, bf0 = len(ba.bp_iterations), len(ba.bf16_sweeps)
     with ClockSampler(local) as clk:
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
@@ -619,7 +620,7 @@ def run_anneal(args, world, rank, local):
             "metric": METRIC, "workload": "batched annealing", "value": world * len(energies) * args.steps / elapsed,
             "unit": "instance-steps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": elapsed / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
-            "dtype": "c128", "data": "synthetic",
+            "dtype": "c128" if args.anneal_precision == "fp64" else "bf16 regauge sweeps + c128", "data": "synthetic",
             "config": {"instances": args.instances, "nodes": int(sum(sizes)), "chi": args.chi,
                        "trotter_steps": n_steps, "dt": dt, "order": 2, "bp_accuracy": 1e-5,
                        "bp_schedule": "synchronous, per-instance convergence"},
@@ -627,6 +628,9 @@ def run_anneal(args, world, rank, local):
             "bp_edge_updates_per_s_rank0": upd / elapsed,
             "bp_sweeps_per_regauge_rank0": {"mean": float(np.mean(ba.bp_iterations[sw0:])),
                                             "max": int(np.max(ba.bp_iterations[sw0:]))},
+            "precision": args.anneal_precision,
+            "bf16_sweeps_per_regauge_rank0": (float(np.mean(ba.bf16_sweeps[bf0:])) if ba.bf16_sweeps[bf0:]
+                                              else None),
             "clocks": clk.summary(),
         }), flush=True)
 
@@ -785,6 +789,8 @@ def main():
     ap.add_argument("--grad-nodes", type=int, default=512)
     ap.add_argument("--instances", type=int, default=64)
     ap.add_argument("--chi", type=int, default=8)
+    ap.add_argument("--anneal-precision", choices=["fp64", "mixed"], default="fp64",
+                    help="batched annealing: plain FP64, or BF16 tensor-core regauge sweeps handing over to FP64")
     ap.add_argument("--trotter-steps", type=int, default=200)
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)

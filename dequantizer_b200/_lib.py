@@ -90,6 +90,7 @@ _SIGNATURES = {
     "dqz_pack_bf16_planes": (ctypes.c_int, [_G, _P, _P, _P]),
     "dqz_messages_distance": (ctypes.c_int, [_G, _P, _P, _P, _P, _P, _P, _I, _P]),
     "dqz_reduce_sum": (ctypes.c_int, [_P, _I, _D, _P, _P]),
+    "dqz_message_changes_c64": (ctypes.c_int, [_G, _P, _P, _P, _P]),
     "dqz_segment_distance": (ctypes.c_int, [_P, _P, _P, _I, _P, _P, _P]),
     "dqz_bp_node_vjp": (ctypes.c_int, [_G, _P, _P, _P, _P, _P, _P, _I, _I, _I, _P, _P]),
     "dqz_qr_batched": (ctypes.c_int, [_P, ctypes.c_int64, _I, _I, _P, _P, _P, _P]),

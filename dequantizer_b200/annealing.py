@@ -51,12 +51,31 @@ class BatchedAnnealer:
         schedule: str = "sync",
         key: int = 0,
         autotune: bool = False,
+        precision: str = "fp64",
+        bf16_handover: float = 2e-4,
+        bf16_max_sweeps: int = 40,
     ):
         """``autotune``: time the gauge kernels' launch shapes on the first
         regauge of every new maximal bond dimension (``autotune.tune_gauge``,
-        cached on disk) and use the fastest."""
+        cached on disk) and use the fastest.
+
+        ``precision="mixed"``: once every bond has dimension 16, each regauge
+        first runs BF16 tensor-core sweeps (dqz_bp_node_update_k3_umma, FP32
+        accumulation, complex64 messages) on the instances above the accuracy,
+        with no gauge or distance evaluation, until an instance's mean change of
+        its node->edge messages per sweep falls to ``bf16_handover`` (at most
+        ``bf16_max_sweeps``); the FP64 loop of the reference (sweep, Vidal gauge,
+        Vidal distance until the accuracy) then finishes from there. Eigen and
+        singular value decompositions, the distances and the gates stay FP64.
+        ``precision="fp64"`` is the plain form."""
         if schedule not in ("sync", "flooding"):
             raise ValueError("batched annealing runs the synchronous or flooding BP schedule")
+        if precision not in ("fp64", "mixed"):
+            raise ValueError("precision must be 'fp64' or 'mixed'")
+        self.precision = precision
+        self.bf16_handover = float(bf16_handover)
+        self.bf16_max_sweeps = int(bf16_max_sweeps)
+        self.bf16_sweeps: List[List[int]] = []
         if not torch.cuda.is_available():
             raise RuntimeError("BatchedAnnealer runs on the GPU only")
         _lib.lib()
@@ -212,6 +231,12 @@ class BatchedAnnealer:
             partial = torch.zeros(max(L.n_halves, 1), dtype=torch.float64, device=dev)
         iters = np.zeros(self.n_inst, dtype=np.int64)
         vd_h = vd.cpu().numpy()
+        if self.precision == "mixed" and L.uniform_k3_chi() == 16:
+            todo = vd_h > self.accuracy
+            if self.max_iters is not None:
+                todo &= self.max_iters > 0
+            if todo.any():
+                n2e, e2n = self._bf16_prephase(T, n2e, e2n, todo)
         while True:
             active = vd_h > self.accuracy
             if self.max_iters is not None:
@@ -235,6 +260,46 @@ class BatchedAnnealer:
         self.bp_iterations.append(iters.tolist())
         self.vidal_distances.append(vd_h.copy())
         return G, lam
+
+    def _bf16_prephase(self, T, n2e, e2n, active: np.ndarray):
+        """BF16 tensor-core sweeps of the listed instances (complex64 messages)
+        until each one's mean node->edge message change per sweep is at most
+        ``bf16_handover``; returns complex128 message arenas for the FP64 loop.
+        Instances not listed keep their messages."""
+        L = self.layout
+        dev = L.device
+        stream = _lib.stream_handle()
+        src_sel, edge_new, _ = self.topo.device_tables(dev)
+        per_node = int(_lib.lib().dqz_bf16_umma_elems_per_node())
+        if getattr(self, "_T_bf16", None) is None or self._T_bf16.numel() != L.n_nodes * per_node:
+            self._T_bf16 = torch.empty(L.n_nodes * per_node, dtype=torch.bfloat16, device=dev)
+            self._halves_per_inst = torch.from_numpy(
+                (self.half_bounds[:, 1] - self.half_bounds[:, 0]).astype(np.float64)).to(dev)
+        T32 = T.to(torch.complex64)
+        _lib.call("dqz_pack_bf16_umma", L.gptr, T32.data_ptr(), self._T_bf16.data_ptr(), stream)
+        a, b = n2e.to(torch.complex64), e2n.to(torch.complex64)
+        flag = error_flag(dev)
+        change = torch.empty(max(L.n_halves, 1), dtype=torch.float64, device=dev)
+        sweeps = np.zeros(self.n_inst, dtype=np.int64)
+        active = active.copy()
+        for _ in range(self.bf16_max_sweeps):
+            nodes = torch.from_numpy(self._ranges(self.node_bounds, active)).to(dev)
+            a_new, b_new = a.clone(), torch.empty_like(b)
+            _lib.call("dqz_bp_node_update_k3_umma", L.gptr, self._T_bf16.data_ptr(), a.data_ptr(), b.data_ptr(),
+                      a_new.data_ptr(), src_sel.data_ptr(), nodes.data_ptr(), nodes.numel(), flag.data_ptr(), stream)
+            _lib.call("dqz_bp_edge_pass_c64", L.gptr, a.data_ptr(), a_new.data_ptr(), edge_new.data_ptr(),
+                      b_new.data_ptr(), stream)
+            _lib.call("dqz_message_changes_c64", L.gptr, a_new.data_ptr(), a.data_ptr(), change.data_ptr(), stream)
+            sums = torch.zeros(self.n_inst, dtype=torch.float64, device=dev)
+            sums.index_add_(0, self.inst_id_half, change[: L.n_halves])
+            mean_change = (sums / self._halves_per_inst).cpu().numpy()
+            a, b = a_new, b_new
+            sweeps += active
+            active &= mean_change > self.bf16_handover
+            if not active.any():
+                break
+        self.bf16_sweeps.append(sweeps.tolist())
+        return a.to(torch.complex128), b.to(torch.complex128)
 
     def _sweep_halves(self, T, n2e, e2n, n2e_new, e2n_new, halves):
         """One synchronous / flooding sweep on the listed half-edges (n2e_new

@@ -212,6 +212,29 @@ __global__ void msg_dist_kernel(dqz_graph_t g, const cd *n2e_a, const cd *n2e_b,
   }
 }
 
+// partial[h] = |a[h] - b[h]|_F over the node->edge messages of complex64 arenas.
+__global__ void msg_dist_c64_kernel(dqz_graph_t g, const float2 *a, const float2 *b, double *partial) {
+  const int nh = g.n_halves;
+  const int wpb = blockDim.x >> 5;
+  const int lane = threadIdx.x & 31;
+  for (int h = blockIdx.x * wpb + (threadIdx.x >> 5); h < nh; h += gridDim.x * wpb) {
+    const int e = g.half_edge[h];
+    if (e < 0) {
+      if (lane == 0) partial[h] = 0.0;
+      continue;
+    }
+    const int c = g.edge_chi[e];
+    const float2 *A = a + g.half_msg_off[h], *B = b + g.half_msg_off[h];
+    double acc = 0.0;
+    for (int i = lane; i < c * c; i += 32) {
+      const double dx = (double)A[i].x - (double)B[i].x, dy = (double)A[i].y - (double)B[i].y;
+      acc += dx * dx + dy * dy;
+    }
+    acc = warp_sum(acc);
+    if (lane == 0) partial[h] = sqrt(acc);
+  }
+}
+
 // out[0] = sum(partial[0..n)) * scale, deterministic single-CTA reduction.
 __global__ void reduce_sum_kernel(const double *partial, int n, double scale, double *out) {
   __shared__ double red[48];
@@ -333,5 +356,17 @@ extern "C" int dqz_bp_sweep_levels(const dqz_graph_t *g, const void *tensors, co
                          (int)n_levels, (int)max_slice, (int)max_chi, (unsigned *)sync, (int *)error_flag) !=
       cudaSuccess)
     return DQZ_ERR_CUDA;
+  return DQZ_OK;
+}
+
+extern "C" int dqz_message_changes_c64(const dqz_graph_t *g, const void *n2e_a, const void *n2e_b, double *partial,
+                                       cudaStream_t stream) {
+  if (!g || !n2e_a || !n2e_b || !partial) return DQZ_ERR_ARG;
+  const int nh = g->n_halves;
+  if (nh == 0) return DQZ_OK;
+  const int wpb = 8;
+  msg_dist_c64_kernel<<<(nh + wpb - 1) / wpb, wpb * 32, 0, stream>>>(*g, (const float2 *)n2e_a, (const float2 *)n2e_b,
+                                                                   partial);
+  DQZ_CHECK_LAUNCH();
   return DQZ_OK;
 }

@@ -176,6 +176,12 @@ int dqz_messages_distance(const dqz_graph_t *g, const void *n2e_a, const void *n
                           const void *e2n_a, const void *e2n_b, double *partial, double *out,
                           int32_t max_chi, cudaStream_t stream);
 
+/* partial[h] = |n2e_a[h] - n2e_b[h]|_F for every half-edge, complex64 arenas
+ * (the per-message terms of mappings/messages_distance.py:14-22 over the
+ * node->edge messages; the batched annealer sums them per instance). */
+int dqz_message_changes_c64(const dqz_graph_t *g, const void *n2e_a, const void *n2e_b, double *partial,
+                            cudaStream_t stream);
+
 /* out[0] = scale * sum(partial[0..n)), deterministic single-CTA reduction. */
 int dqz_reduce_sum(const double *partial, int32_t n, double scale, double *out, cudaStream_t stream);
 

@@ -15,6 +15,7 @@ import torch
 
 from dequantizer_b200 import workloads as W
 from dequantizer_b200 import graph as G
+from dequantizer_b200 import maps as M
 from dequantizer_b200.graph import Edge, Node
 from dequantizer_b200.initializers import get_message_random_nonnegative_initializer, get_potts_initializer
 from oracle import maps as OM
@@ -184,3 +185,25 @@ def test_batched_measurement_sampling_equals_independent_runs():
                                      synchronous_update=True, sample_measurements=True, samples=U[k])
         assert np.array_equal(spin_configs[k], res.configuration)
         assert set(np.unique(spin_configs[k])) <= {-1, 1}
+
+
+def test_mixed_precision_batched_annealer_tracks_fp64():
+    """BatchedAnnealer(precision="mixed"): once every bond has dimension 16,
+    each regauge starts with BF16 tensor-core sweeps and hands over to the
+    FP64 loop of the reference; the densities stay within 1e-4 of the FP64
+    annealer's (the FP64 loop finishes every regauge to the same accuracy)."""
+    from dequantizer_b200.annealing import BatchedAnnealer
+
+    energies = [W.random_regular_energy(n, 3, seed=60 + n, field_std=0.5) for n in (16, 20, 24)]
+    steps = list(W.scheduler(0.5, lambda t: 1 - t, 10))
+    runs = {}
+    for prec in ("fp64", "mixed"):
+        ba = BatchedAnnealer(energies, max_chi=16, accuracy=1e-7, max_belief_propagation_iterations=200,
+                             precision=prec)
+        runs[prec] = (ba.run(steps, second_order=True), ba)
+    mixed = runs["mixed"][1]
+    assert mixed.layout.uniform_k3_chi() == 16
+    assert sum(sum(s) for s in mixed.bf16_sweeps) > 0, "no regauge took the BF16 path"
+    for k in range(len(energies)):
+        assert np.abs(runs["mixed"][0][k] - runs["fp64"][0][k]).max() < 1e-4
+    assert int(M.error_flag(torch.device("cuda", 0)).item()) == 0
