@@ -273,7 +273,7 @@ __host__ __device__ inline size_t su_scratch_per_job(int max_rows, int max_cols)
 __global__ void __launch_bounds__(GATE_THREADS) simple_update_kernel(
     dqz_graph_t g, cd *Tall, double *lambdas, const int32_t *edges, const uint8_t *ctrl_first, const cd *halves,
     const int32_t *ranks, int n, double eps, int max_rank, int max_rows, int max_cols, double *err_out,
-    double *ent_out, cd *scratch, long long fused_cap) {
+    double *ent_out, cd *scratch, const uint8_t *done) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double *red = reinterpret_cast<double *>(smem_raw);
   int *flag = reinterpret_cast<int *>(red + 48);
@@ -295,7 +295,7 @@ __global__ void __launch_bounds__(GATE_THREADS) simple_update_kernel(
     su_load_side(g, lambdas, hu, U);
     su_load_side(g, lambdas, hv, V);
     const int r = ranks[j];
-    if (suf_fits(U, V, r, max_rank, fused_cap)) continue;  // done by the shared-memory form
+    if (done && done[j]) continue;  // done by the on-chip form (its marks, taken on the original shapes)
     const int ce = U.dims[U.slot];
     const int K = ce * r;
     cd *Au = scratch + (size_t)blockIdx.x * (su_scratch_per_job(max_rows, max_cols) / sizeof(cd));
@@ -418,7 +418,7 @@ constexpr size_t SUF_SMEM_MAX = 220 * 1024;  // dynamic shared memory per CTA (p
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(SUF_THREADS, 1)
     simple_update_onchip_kernel(dqz_graph_t g, cd *Tall, double *lambdas, const int32_t *edges,
                                 const uint8_t *ctrl_first, const cd *halves, const int32_t *ranks, int n, double eps,
-                                int max_rank, double *err_out, double *ent_out, long long cap) {
+                                int max_rank, double *err_out, double *ent_out, long long cap, uint8_t *done) {
   namespace cg = cooperative_groups;
   cg::cluster_group cluster = cg::this_cluster();
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -439,7 +439,12 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(SUF_THREADS, 1)
     su_load_side(g, lambdas, hu, U);
     su_load_side(g, lambdas, hv, V);
     const int r = ranks[j];
-    if (!suf_fits(U, V, r, max_rank, cap)) continue;  // left to the global-scratch kernel; same decision in both CTAs
+    // decided on the job's shapes before any update; the mark tells the
+    // global-scratch kernel (launched next) which jobs are done, since this
+    // launch changes the bond dimensions the decision reads
+    const bool fits = suf_fits(U, V, r, max_rank, cap);
+    if (side == 0 && threadIdx.x == 0) done[j] = fits ? 1 : 0;
+    if (!fits) continue;  // left to the global-scratch kernel; same decision in both CTAs
     const SUSide &X = side ? V : U;
     SufDims D, Du, Dv;
     suf_dims(U, r, Du);
@@ -697,9 +702,14 @@ extern "C" int dqz_apply_half_gates(const void *tensors_in, void *tensors_out, c
   return DQZ_OK;
 }
 
+// Scratch of dqz_simple_update: one byte per job (which jobs the on-chip form
+// did), rounded up to 256 bytes, then one slice per CTA of the global-scratch
+// kernel.
+__host__ __device__ inline size_t su_marks_bytes(int32_t n) { return ((size_t)n + 255) & ~(size_t)255; }
+
 extern "C" size_t dqz_simple_update_scratch_bytes(int32_t n, int32_t max_rows, int32_t max_cols) {
   int grid = n < SU_GRID_MAX ? n : SU_GRID_MAX;
-  return (size_t)grid * su_scratch_per_job(max_rows, max_cols);
+  return su_marks_bytes(n) + (size_t)grid * su_scratch_per_job(max_rows, max_cols);
 }
 
 extern "C" int dqz_simple_update(const dqz_graph_t *g, void *tensors, double *lambdas, const int32_t *edges,
@@ -716,17 +726,19 @@ extern "C" int dqz_simple_update(const dqz_graph_t *g, void *tensors, double *la
   // jobs of A matrices with 256 rows or more (bond 16 and up between degree-3
   // nodes) go to the on-chip form where they fit; the global-scratch kernel
   // below then takes only the others
-  long long fused_cap = 0;
-  if (max_rows >= SUF_MIN_ROWS) {
+  uint8_t *marks = nullptr;
+  cd *job_scratch = reinterpret_cast<cd *>(static_cast<char *>(scratch) + su_marks_bytes(n));
+  if (max_rows >= SUF_MIN_ROWS && dqz_get_tuning(DQZ_TUNE_SU_ONCHIP) != 1) {
     DQZ_SMEM_ATTR_ONCE(simple_update_onchip_kernel, SUF_SMEM_MAX);
-    fused_cap = (long long)(SUF_SMEM_MAX / sizeof(cd));
+    const long long cap = (long long)(SUF_SMEM_MAX / sizeof(cd));
+    marks = static_cast<uint8_t *>(scratch);
     int dev = 0, sms = 148;
     if (cudaGetDevice(&dev) != cudaSuccess) return DQZ_ERR_CUDA;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const int pairs = n < sms / 2 ? n : sms / 2;  // one CTA per SM, two per cluster
     simple_update_onchip_kernel<<<2 * pairs, SUF_THREADS, SUF_SMEM_MAX, stream>>>(
         *g, (cd *)tensors, lambdas, edges, ctrl_is_first, (const cd *)halves, ranks, n, eps, max_rank, err, entropy,
-        fused_cap);
+        cap, marks);
     DQZ_CHECK_LAUNCH();
   }
   DQZ_SMEM_ATTR_ONCE(simple_update_kernel, SMEM_LIMIT);
@@ -735,7 +747,7 @@ extern "C" int dqz_simple_update(const dqz_graph_t *g, void *tensors, double *la
   if (tuned > 0 && tuned < grid) grid = tuned;
   simple_update_kernel<<<grid, GATE_THREADS, smem, stream>>>(*g, (cd *)tensors, lambdas, edges, ctrl_is_first,
                                                              (const cd *)halves, ranks, n, eps, max_rank, max_rows,
-                                                             max_cols, err, entropy, (cd *)scratch, fused_cap);
+                                                             max_cols, err, entropy, job_scratch, marks);
   DQZ_CHECK_LAUNCH();
   return DQZ_OK;
 }
@@ -799,7 +811,7 @@ extern "C" int dqz_simple_update_noalloc(const dqz_graph_t *g, void *tensors, do
   DQZ_SMEM_ATTR_ONCE(simple_update_kernel, SMEM_LIMIT);
   simple_update_kernel<<<grid, GATE_THREADS, smem, stream>>>(*g, (cd *)tensors, lambdas, edges, ctrl_is_first,
                                                              (const cd *)halves, ranks, n, eps, max_rank, max_rows,
-                                                             max_cols, err, entropy, (cd *)scratch, 0ll);
+                                                             max_cols, err, entropy, (cd *)scratch, nullptr);
   DQZ_CHECK_LAUNCH();
   return DQZ_OK;
 }

@@ -89,6 +89,52 @@ def test_simple_update_at_production_shapes(chi, kind, accuracy, max_rank):
         g_l[edge.id] = torch.from_numpy(r_l[edge.id].copy()).cuda()
 
 
+@pytest.mark.parametrize("path", ["onchip", "global_scratch"])
+@pytest.mark.parametrize("max_rank", [None, 12])
+def test_simple_update_on_uneven_shapes(path, max_rank):
+    """Degree-2 and degree-3 nodes with uneven bonds (the heavy-hex cell with
+    bonds of 2, 8 and 16): jobs whose matrices have 256 rows or more on one
+    side only, wide and tall factors, with and without a rank cap, through the
+    on-chip form (default) and through the global-scratch kernel (knob
+    su_onchip = 1), each against the oracle."""
+    from dequantizer_b200 import autotune
+
+    rng = np.random.default_rng(7 if max_rank else 8)
+    g_ref = G.get_heavy_hex_ibm_eagle_lattice_infinite()
+    g_gpu = G.get_heavy_hex_ibm_eagle_lattice_infinite()
+    dims = {eid: int(rng.choice([2, 8, 16])) for eid in g_ref.edges}
+    for gg in (g_ref, g_gpu):
+        for eid, e in gg.edges.items():
+            e.dimension = dims[eid]
+        gg.refresh_bond_shapes()
+    tensors = random_tensors(g_ref, 41)
+    lambdas = vidal_like_lambdas(g_ref, rng)
+    r_t, r_l = dict(tensors), dict(lambdas)
+    g_t = {k: torch.from_numpy(v).cuda() for k, v in tensors.items()}
+    g_l = {k: torch.from_numpy(v.copy()).cuda() for k, v in lambdas.items()}
+    autotune.set_knobs({"su_onchip": 1 if path == "global_scratch" else 0})
+    try:
+        for a, b in list(g_ref.edges)[:8]:
+            gate = zz_gate(rng) if rng.uniform() < 0.5 else unitary_gate(rng)
+            edge = g_ref.find_edge(a, b)
+            n1, n2 = g_ref.get_node(a), g_ref.get_node(b)
+            if edge.dimension * 4 > 64:
+                gate = zz_gate(rng)  # bond x gate rank stays within the kernels' 64 columns
+            _, _, er, en = OM.apply2_to_vidal_canonical(g_ref, a, b, r_t, r_l, gate, 1e-10, None, max_rank)
+            _, _, eg, ng = g_gpu.apply2_to_vidal_canonical(a, b, g_t, g_l, gate, 1e-10, None, max_rank)
+            assert g_gpu.find_edge(a, b).dimension == edge.dimension
+            assert tuple(g_t[a].shape) == r_t[a].shape and tuple(g_t[b].shape) == r_t[b].shape
+            assert rel_err(g_l[edge.id], r_l[edge.id]) < TOL_SVD
+            assert abs(float(eg) - er) < 1e-10 and abs(float(ng) - en) < 1e-10
+            i1, i2 = n1.indices[edge.id], n2.indices[edge.id]
+            assert rel_err(two_site(g_t[a], g_t[b], i1, i2, g_l[edge.id]),
+                           two_site(r_t[a], r_t[b], i1, i2, r_l[edge.id])) < TOL_SVD
+            g_t[a], g_t[b] = torch.from_numpy(r_t[a]).cuda(), torch.from_numpy(r_t[b]).cuda()
+            g_l[edge.id] = torch.from_numpy(r_l[edge.id].copy()).cuda()
+    finally:
+        autotune.set_knobs({"su_onchip": 0})
+
+
 def heavy_hex_cell_at(chi):
     g = G.get_heavy_hex_ibm_eagle_lattice_infinite()
     for e in g.edges.values():

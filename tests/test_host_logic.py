@@ -41,7 +41,9 @@ def test_scratch_queries_are_host_only():
     lib = _lib.lib()
     assert lib.dqz_bp_node_scratch_bytes(3072, 512, 16) == 0
     assert lib.dqz_bp_node_scratch_bytes(100, 65536, 32) > 0
-    assert lib.dqz_simple_update_scratch_bytes(10, 2048, 64) == 10 * 64 * 2048 * 64
+    # one byte per job (rounded up to 256) marking the on-chip jobs, then a
+    # 64 * rows * cols slice per CTA of the global-scratch kernel
+    assert lib.dqz_simple_update_scratch_bytes(10, 2048, 64) == 256 + 10 * 64 * 2048 * 64
     assert lib.dqz_absorb_scratch_bytes(127, 8192) > 0
 
 
