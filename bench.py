@@ -478,6 +478,119 @@ def bf16_sweep_accuracy(g, packed_c64, m, sweeps):
     return float((z["bf16"] - z["fp64"]).abs().max())
 
 
+def _events_time(fn):
+    """(result, seconds) of fn() between CUDA events on the current stream."""
+    import torch
+
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    s.record()
+    out = fn()
+    e.record()
+    e.synchronize()
+    return out, s.elapsed_time(e) * 1e-3
+
+
+def workload_suite(args):
+    """Bounded runs of the other workloads, reported as extra keys of the
+    default line (each names its sample; none is the headline):
+    * ising3d -- the 3-D Ising canonicalisation in full (6x6x6 open lattice,
+      chi 2, five betas, Vidal distance <= 1e-10; asynchronous DFS sweeps, one
+      cooperative launch each), BP iterations/s, and the oracle's iteration
+      (numpy, one core) timed on a few iterations of the same loop;
+    * anneal -- 64 instances (n ~ U{100..1000} even, J = +-1), chi 16,
+      second-order steps at s = 0.5 from the |+> state (warm-up steps first, so
+      every bond is at 16), FP64 and mixed precision, instance-steps/s;
+      the densities of both forms after the timed steps compared;
+    * eagle -- the 127-qubit kicked-Ising run's first Trotter steps (bonds
+      growing towards 32), Trotter steps/s."""
+    import torch
+
+    from dequantizer_b200.annealing import BatchedAnnealer
+    from dequantizer_b200.workloads import ising_sqrt_partition, random_regular_energy, run_eagle_simulation
+
+    out = {}
+    # ---- 3-D Ising canonicalisation (config 1)
+    betas = [0.1, 0.2, 0.3, 0.4, 0.5]
+    kw = dict(lattice_sizes=[6, 6, 6], betas=betas, coupling=-1.0, field_strength=0.5, accuracy=1e-10,
+              open_boundary=True, synchronous_update=False, key=42, traversal_type="dfs", max_iterations=500)
+    ising_sqrt_partition(**kw)
+    res, dt = _events_time(lambda: ising_sqrt_partition(**kw))
+    iters = int(sum(res.number_of_iterations))
+    out["ising3d"] = {"unit": "BP iterations/s", "value": iters / dt, "iterations_per_scan": iters, "scan_s": dt,
+                      "average_magnetization": [float(x) for x in res.average_magnetization],
+                      "cpu_oracle_iterations_per_s": _ising_oracle_rate(), "cpu_cores": 1}
+    # ---- batched annealing, 64 instances, chi 16, mid-schedule (config 4)
+    rng = np.random.default_rng(0)
+    sizes = [int(2 * rng.integers(50, 501)) for _ in range(64)]
+    energies = [random_regular_energy(n, 3, seed=1000 + i) for i, n in enumerate(sizes)]
+    dt_step, s_mid = 0.1, 0.5
+    anneal = {"instances": 64, "nodes": int(sum(sizes)), "chi": 16, "s": s_mid, "dt": dt_step,
+              "warmup_steps": args.suite_anneal_warmup, "timed_steps": args.suite_anneal_steps,
+              "sample": "second-order steps at s = 0.5 from the |+> state after the warm-up steps (every bond at "
+                        "16), not the annealed trajectory"}
+    rho = {}
+    for prec in ("fp64", "mixed"):
+        ba = BatchedAnnealer(energies, max_chi=16, accuracy=1e-5, max_belief_propagation_iterations=100,
+                             precision=prec)
+        for i in range(args.suite_anneal_warmup):
+            ba.step(-dt_step * (1 - s_mid), dt_step * s_mid, first=(i == 0), second_order=True)
+        n0, b0 = len(ba.bp_iterations), len(ba.bf16_sweeps)
+
+        def steps():
+            for _ in range(args.suite_anneal_steps):
+                ba.step(-dt_step * (1 - s_mid), dt_step * s_mid, first=False, second_order=True)
+
+        _, dt = _events_time(steps)
+        rho[prec] = ba.densities()
+        anneal[prec] = {"unit": "instance-steps/s", "value": 64 * args.suite_anneal_steps / dt,
+                        "ms_per_step": dt / args.suite_anneal_steps * 1e3,
+                        "uniform_bond_16": bool(ba.layout.uniform_k3_chi() == 16),
+                        "fp64_sweeps_per_regauge": float(np.mean(ba.bp_iterations[n0:])),
+                        "bf16_sweeps_per_regauge": (float(np.mean(ba.bf16_sweeps[b0:])) if ba.bf16_sweeps[b0:]
+                                                    else 0.0)}
+        del ba
+        torch.cuda.empty_cache()
+    anneal["mixed_over_fp64"] = anneal["mixed"]["value"] / anneal["fp64"]["value"]
+    dz = max(float(np.abs((a[:, 0, 0] - a[:, 1, 1]).real - (b[:, 0, 0] - b[:, 1, 1]).real).max())
+             for a, b in zip(rho["mixed"], rho["fp64"]))
+    anneal["max_abs_dZ_mixed_vs_fp64"] = dz
+    out["anneal"] = anneal
+    # ---- kicked Ising on the 127-qubit heavy-hex lattice (config 3), first steps
+    n_eagle = args.suite_eagle_steps
+    (z, em), dt = _events_time(lambda: run_eagle_simulation(
+        max_chi=32, layers_per_regauging=1, trotter_steps=n_eagle, accuracy=1e-5, theta=0.6, is_infinite=False,
+        colour_classes=True, all_qubits=True))
+    out["eagle"] = {"unit": "Trotter steps/s", "value": n_eagle / dt, "steps": n_eagle,
+                    "max_bond": int(em._layout.edge_chi.max()),
+                    "sample": f"the first {n_eagle} of the 20 steps (bonds growing towards 32)"}
+    return out
+
+
+def _ising_oracle_rate(iterations=3):
+    """The oracle's canonicalisation iteration (asynchronous DFS sweep, Vidal
+    gauge, Vidal distance; numpy FP64, one process) on the 6x6x6 lattice at
+    beta = 0.3: iterations/s over a few iterations."""
+    from dequantizer_b200.graph import get_nd_lattice
+    from dequantizer_b200.initializers import get_message_random_nonnegative_initializer, get_potts_initializer
+    from oracle import maps as OM
+
+    lat = get_nd_lattice([6, 6, 6], 2, 2, True)
+    trav = list(lat.get_traversal_iterator(ordering="dfs"))
+    bp, vg, vd = (OM.get_belief_propagation_map(trav), OM.get_vidal_gauge_fixing_map(trav, 1e-10),
+                  OM.get_vidal_gauge_distance_map(trav, 1e-10))
+    spins = np.array([1.0, -1.0])
+    init = get_potts_initializer(np.exp(0.3 * np.tensordot(spins, spins, axes=0)), np.exp(-0.15 * spins))
+    tensors = OM.init_tensors(lat, init)
+    msgs = lat.init_messages(get_message_random_nonnegative_initializer(42))
+    t0 = time.perf_counter()
+    for _ in range(iterations):
+        msgs = bp(tensors, msgs)
+        t, lam = vg(tensors, msgs)
+        vd(t, lam)
+    return iterations / (time.perf_counter() - t0)
+
+
 def run_ours(args, world, rank, local):
     import torch
 
@@ -540,6 +653,12 @@ def run_ours(args, world, rank, local):
             cpu_v, cores, sample = cpu.sample(args.cpu_seconds)
         # one worker process with one BLAS thread: the single-core figure
         cpu1, _, _ = CpuBaseline.single(tensors, m, min(4.0, args.cpu_seconds))
+    suite = None
+    if world == 1 and not args.no_suite:
+        try:
+            suite = workload_suite(args)
+        except Exception as exc:  # an auxiliary block: report it, keep the headline line
+            suite = {"error": f"{type(exc).__name__}: {exc}"}
     line = {
         "metric": METRIC, "value": rbf["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": rbf["ms_per_step"], "higher_is_better": True,
@@ -566,6 +685,7 @@ def run_ours(args, world, rank, local):
                 "d2h_bytes_per_step": rbf["d2h"]},
         "gpu_launches": rbf["launches"],
         "clocks": clk.summary(),
+        "other_workloads": suite,
     }
     print(json.dumps(line), flush=True)
 
@@ -799,6 +919,10 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--ref-seconds", type=float, default=4.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-suite", action="store_true", help="skip the bounded runs of the other workloads")
+    ap.add_argument("--suite-anneal-warmup", type=int, default=6)
+    ap.add_argument("--suite-anneal-steps", type=int, default=4)
+    ap.add_argument("--suite-eagle-steps", type=int, default=6)
     ap.add_argument("--e2e-chunks", type=int, default=8,
                     help="node ranges the end-to-end sweep streams its host inputs in (1: no overlap)")
     ap.add_argument("--no-accuracy", action="store_true")
