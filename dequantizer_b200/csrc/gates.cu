@@ -483,7 +483,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(SUF_THREADS, 1)
       }
       __syncthreads();
     }
-    householder_qr(Bm, D.MB, D.KB, tauB, red);
+    householder_qr_owned(Bm, D.MB, D.KB, tauB);
 
     // ---- S[(c, o), (a, rho)] = sum_i R_B[c, (a, i)] h[rho][o][i], normalised (|A|_F = |S|_F)
     {
@@ -505,7 +505,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(SUF_THREADS, 1)
       for (long long idx = tid; idx < total; idx += nt) Sm[idx] = cscale(Sm[idx], inv);
       __syncthreads();
     }
-    householder_qr(Sm, D.MS, D.KS, tauS, red);
+    householder_qr_owned(Sm, D.MS, D.KS, tauS);
 
     // ---- swap R_S: the partner's R (muS x K, upper trapezoidal) into W, then the core
     cluster.sync();

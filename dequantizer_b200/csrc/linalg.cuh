@@ -330,6 +330,57 @@ static __device__ void householder_qr(cd *A, int M, int K, cd *tau, double *red)
   }
 }
 
+// The same factorisation (same reflector convention) with one barrier per
+// column: warp w owns the columns c with c % (warps) == w. After applying
+// reflector j to its columns, the owner of column j + 1 builds reflector j + 1
+// from that column at once (norm by a warp reduction, zlarfg's beta and tau),
+// so the next barrier publishes both. For matrices in shared memory.
+__device__ __forceinline__ void qr_make_reflector(cd *A, int M, int j, cd *tau) {
+  const int lane = threadIdx.x & 31;
+  cd *col = A + (long long)j * M;
+  double s = 0.0;
+  for (int r = j + 1 + lane; r < M; r += 32) s += cabs2(col[r]);
+  s = warp_sum(s);
+  const cd alpha = col[j];
+  cd t = czero();
+  if (!(s == 0.0 && alpha.y == 0.0)) {
+    const double beta = -copysign(sqrt(cabs2(alpha) + s), alpha.x);
+    t = mk((beta - alpha.x) / beta, -alpha.y / beta);
+    const cd sc = cdiv(mk(1.0, 0.0), mk(alpha.x - beta, alpha.y));
+    for (int r = j + 1 + lane; r < M; r += 32) col[r] = cmul(col[r], sc);
+    __syncwarp();
+    if (lane == 0) col[j] = mk(beta, 0.0);
+  }
+  if (lane == 0) tau[j] = t;
+  __syncwarp();
+}
+
+static __device__ void householder_qr_owned(cd *A, int M, int K, cd *tau) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int kk = M < K ? M : K;
+  if (kk > 0 && warp == 0) qr_make_reflector(A, M, 0, tau);
+  __syncthreads();
+  for (int j = 0; j < kk; ++j) {
+    const cd t = tau[j];
+    const cd *v = A + (long long)j * M;
+    for (int c = j + 1 + ((warp - (j + 1) % nw + nw) % nw); c < K; c += nw) {  // this warp's columns > j
+      if (t.x != 0.0 || t.y != 0.0) {
+        cd *ac = A + (long long)c * M;
+        cd w = czero();
+        if (lane == 0) w = ac[j];
+        for (int r = j + 1 + lane; r < M; r += 32) cfmac(w, v[r], ac[r]);
+        w = warp_csum(w);
+        const cd f = cmulc(t, w);  // conj(tau) * w
+        if (lane == 0) ac[j] = csub(ac[j], f);
+        for (int r = j + 1 + lane; r < M; r += 32) ac[r] = csub(ac[r], cmul(v[r], f));
+        __syncwarp();
+      }
+      if (c == j + 1 && j + 1 < kk) qr_make_reflector(A, M, j + 1, tau);
+    }
+    __syncthreads();
+  }
+}
+
 // X <- Q X with Q = H_0 ... H_{kk-1} from householder_qr; X is M x p,
 // column-major (ldx).
 static __device__ void apply_q(const cd *A, int M, int kk, const cd *tau, cd *X, int ldx, int p) {
