@@ -310,8 +310,8 @@ __global__ void __launch_bounds__(GATE_THREADS) simple_update_kernel(
 
     su_build(U, Tu, Hu, r, Au, red);
     su_build(V, Tv, Hv, r, Av, red);
-    householder_qr(Au, U.M, K, tau_u, red);
-    householder_qr(Av, V.M, K, tau_v, red);
+    householder_qr_owned(Au, U.M, K, tau_u);
+    householder_qr_owned(Av, V.M, K, tau_v);
     const int mu = U.M < K ? U.M : K;
     const int mv = V.M < K ? V.M : K;
     const int kk = mu < mv ? mu : mv;

@@ -21,7 +21,6 @@ __global__ void __launch_bounds__(QR_THREADS) qr_batched_kernel(const cd *__rest
                                                                 int k, cd *Q, cd *R, cd *scratch) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cd *tau = reinterpret_cast<cd *>(smem_raw);
-  __shared__ double red[48];
   const int kk = m < k ? m : k;
   const int tid = threadIdx.x, nt = blockDim.x;
   cd *W = scratch + (long long)blockIdx.x * (qr_scratch_per_matrix(m, k) / sizeof(cd));
@@ -33,7 +32,7 @@ __global__ void __launch_bounds__(QR_THREADS) qr_batched_kernel(const cd *__rest
       W[(long long)j * m + i] = Ab[idx];
     }
     __syncthreads();
-    householder_qr(W, m, k, tau, red);
+    householder_qr_owned(W, m, k, tau);
     cd *Rb = R + b * (long long)kk * k;
     for (int idx = tid; idx < kk * k; idx += nt) {
       const int i = idx / k, j = idx - (idx / k) * k;
