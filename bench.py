@@ -524,17 +524,18 @@ def workload_suite(args):
     rng = np.random.default_rng(0)
     sizes = [int(2 * rng.integers(50, 501)) for _ in range(64)]
     energies = [random_regular_energy(n, 3, seed=1000 + i) for i, n in enumerate(sizes)]
-    dt_step, s_mid = 0.1, 0.5
+    dt_step, s_mid, dt_warm = 0.1, 0.5, args.suite_anneal_warm_dt
     anneal = {"instances": 64, "nodes": int(sum(sizes)), "chi": 16, "s": s_mid, "dt": dt_step,
               "warmup_steps": args.suite_anneal_warmup, "timed_steps": args.suite_anneal_steps,
-              "sample": "second-order steps at s = 0.5 from the |+> state after the warm-up steps (every bond at "
-                        "16), not the annealed trajectory"}
+              "warmup_dt": dt_warm,
+              "sample": "second-order steps (dt 0.1) at s = 0.5 from the |+> state after warm-up steps of a larger dt "
+                        "that entangle the state (every bond at 16, regauges that sweep), not the annealed trajectory"}
     rho = {}
     for prec in ("fp64", "mixed"):
         ba = BatchedAnnealer(energies, max_chi=16, accuracy=1e-5, max_belief_propagation_iterations=100,
                              precision=prec)
         for i in range(args.suite_anneal_warmup):
-            ba.step(-dt_step * (1 - s_mid), dt_step * s_mid, first=(i == 0), second_order=True)
+            ba.step(-dt_warm * (1 - s_mid), dt_warm * s_mid, first=(i == 0), second_order=True)
         n0, b0 = len(ba.bp_iterations), len(ba.bf16_sweeps)
 
         def steps():
@@ -922,6 +923,7 @@ def main():
     ap.add_argument("--no-suite", action="store_true", help="skip the bounded runs of the other workloads")
     ap.add_argument("--suite-anneal-warmup", type=int, default=6)
     ap.add_argument("--suite-anneal-steps", type=int, default=4)
+    ap.add_argument("--suite-anneal-warm-dt", type=float, default=1.0)
     ap.add_argument("--suite-eagle-steps", type=int, default=6)
     ap.add_argument("--e2e-chunks", type=int, default=8,
                     help="node ranges the end-to-end sweep streams its host inputs in (1: no overlap)")

@@ -247,11 +247,18 @@ __device__ __forceinline__ long long suf_cw(const SufDims &D, int d, int rk) {
   return suf_even(cw > g ? cw : g);
 }
 
+// X region: the kept columns (MS x rk), and before them the R^H work matrix
+// of the core SVD (K x K at most).
+__device__ __forceinline__ long long suf_x(const SufDims &D, int rk) {
+  const long long a = (long long)D.MS * rk, b = (long long)D.KS * D.KS;
+  return suf_even(a > b ? a : b);
+}
+
 // Complex entries of one side's shared-memory layout, in this order:
-//   S [MS*KS] | tauS [muS] | B [MB*KB] | tauB [muB] | core, W [cw] | X [MS*rk]
+//   S [MS*KS] | tauS [muS] | B [MB*KB] | tauB [muB] | core, W [cw] | X [suf_x]
 __device__ __forceinline__ long long suf_need(const SufDims &D, int d, int rk) {
   return suf_even((long long)D.MS * D.KS) + suf_even(D.muS) + suf_even((long long)D.MB * D.KB) + suf_even(D.muB) +
-         suf_cw(D, d, rk) + suf_even((long long)D.MS * rk);
+         suf_cw(D, d, rk) + suf_x(D, rk);
 }
 
 // Whether a job runs in the shared-memory form with `cap` complex entries
@@ -281,7 +288,9 @@ __global__ void __launch_bounds__(GATE_THREADS) simple_update_kernel(
   cd *tau_v = tau_u + max_cols;
   cd *core = tau_v + max_cols;
   cd *W = core + max_cols * max_cols;
-  double *sv = reinterpret_cast<double *>(W + max_cols * max_cols);
+  cd *Xq = W + max_cols * max_cols;  // R^H of the QR-preconditioned core SVD
+  cd *tau_c = Xq + max_cols * max_cols;
+  double *sv = reinterpret_cast<double *>(tau_c + max_cols);
   int *perm = reinterpret_cast<int *>(sv + max_cols);
   int *acc = perm + max_cols;
   __shared__ double lam_sh[2 * DQZ_MAX_CHI];
@@ -329,7 +338,7 @@ __global__ void __launch_bounds__(GATE_THREADS) simple_update_kernel(
         core[i * mv + jj] = cconj(a);
     }
     __syncthreads();
-    hestenes(core, zr, zr, kk, W, kk, sv, flag, red);
+    hestenes_qr(core, zr, kk, W, Xq, tau_c, sv, flag, acc, red);
     sort_desc(sv, kk, perm);
     const int rank = (max_rank > 0 && max_rank < kk) ? max_rank : kk;
     // unit columns of Z; null ones among the `rank` kept are completed below
@@ -390,8 +399,8 @@ __global__ void __launch_bounds__(GATE_THREADS) simple_update_kernel(
 }
 
 size_t su_smem_bytes(int max_cols) {
-  return 48 * sizeof(double) + 4 * sizeof(int) + 2 * (size_t)max_cols * sizeof(cd) +
-         2 * (size_t)max_cols * max_cols * sizeof(cd) + (size_t)max_cols * sizeof(double) +
+  return 48 * sizeof(double) + 4 * sizeof(int) + 3 * (size_t)max_cols * sizeof(cd) +
+         3 * (size_t)max_cols * max_cols * sizeof(cd) + (size_t)max_cols * sizeof(double) +
          2 * (size_t)max_cols * sizeof(int);
 }
 
@@ -427,6 +436,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(SUF_THREADS, 1)
   __shared__ int flag[4];
   __shared__ double sv[DQZ_MAX_CHI], lam_sh[DQZ_MAX_CHI], lam_in[DQZ_MAX_CHI];
   __shared__ int perm[DQZ_MAX_CHI], acc[DQZ_MAX_CHI];
+  __shared__ cd tau_c[DQZ_MAX_CHI];
   const int side = (int)cluster.block_rank();  // 0: controlling node, 1: controlled node
   const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
 
@@ -538,7 +548,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(SUF_THREADS, 1)
         core[i * mv + jj] = cconj(v);
     }
     __syncthreads();
-    hestenes(core, zr, zr, kk, W, kk, sv, flag, red);
+    hestenes_qr(core, zr, kk, W, Xm, tau_c, sv, flag, acc, red);  // Xm is free until X is formed below
     sort_desc(sv, kk, perm);
     const int rank = (max_rank > 0 && max_rank < kk) ? max_rank : kk;
     for (int idx = tid; idx < zr * kk; idx += nt) {

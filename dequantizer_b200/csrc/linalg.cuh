@@ -23,14 +23,18 @@ struct Rot {
 
 // Pair i of round-robin step `step` for an even count np: (0, step+1) for
 // i == 0, otherwise (step+i, step-i) modulo np-1, shifted by one.
+// (step < np - 1 and i < np / 2, so each modulo is one conditional step.)
 __device__ __forceinline__ void rr_pair(int step, int i, int np, int &p, int &q) {
   const int m = np - 1;
   if (i == 0) {
     p = 0;
-    q = step % m + 1;
+    q = step + 1;
   } else {
-    p = (step + i) % m + 1;
-    q = ((step - i) % m + m) % m + 1;
+    int a = step + i, b = step - i;
+    if (a >= m) a -= m;
+    if (b < 0) b += m;
+    p = a + 1;
+    q = b + 1;
   }
   if (p > q) {
     int t = p;
@@ -42,14 +46,18 @@ __device__ __forceinline__ void rr_pair(int step, int i, int np, int &p, int &q)
 // Unitary J = D R that diagonalises the Hermitian 2x2 [[a, c], [conj(c), b]]
 // (a, b real): D = diag(c/|c|, 1), R the real Jacobi rotation of
 // [[a, |c|], [|c|, b]]. Returns false when c is negligible.
+// One reciprocal square root gives both 1/|c| (phase and tau) and no
+// divisions by |c|; cos = 1/sqrt(1 + t^2) is another (FP64 division and
+// square root are long instruction sequences, and this runs per pair and step).
 __device__ __forceinline__ bool jacobi_rot(double a, double b, cd c, Rot &r) {
-  double ac = sqrt(cabs2(c));
-  if (!(ac > 0.0) || ac < 1e-300) return false;
-  double tau = (b - a) / (2.0 * ac);
-  double t = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
-  double cs = 1.0 / sqrt(1.0 + t * t);
-  double sn = t * cs;
-  cd ph = mk(c.x / ac, c.y / ac);
+  const double ac2 = cabs2(c);
+  if (!(ac2 > 1e-300)) return false;
+  const double inv_ac = rsqrt(ac2);
+  const double tau = (b - a) * 0.5 * inv_ac;
+  const double t = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
+  const double cs = rsqrt(1.0 + t * t);
+  const double sn = t * cs;
+  const cd ph = mk(c.x * inv_ac, c.y * inv_ac);
   r.j00 = cscale(ph, cs);
   r.j01 = cscale(ph, sn);
   r.j10 = mk(-sn, 0.0);
@@ -197,8 +205,7 @@ static __device__ void hestenes(cd *A, int lda, int m, int n, cd *V, int ldv, do
           al = warp_sum(al);
           be = warp_sum(be);
           ga = warp_csum(ga);
-          double ag = sqrt(cabs2(ga));
-          if (!(al > null_thr) || !(be > null_thr) || !(ag > tol * sqrt(al) * sqrt(be))) continue;
+          if (!(al > null_thr) || !(be > null_thr) || !(cabs2(ga) > tol * tol * al * be)) continue;
           Rot r;
           if (!jacobi_rot(al, be, ga, r)) continue;
           if (lane == 0) *flag = 1;
@@ -404,6 +411,50 @@ static __device__ void apply_q(const cd *A, int M, int kk, const cd *tau, cd *X,
   }
 }
 
+// hestenes on Z (zr x kk, column-major, ld zr, zr >= kk) with QR
+// preconditioning: Z = Q R (Householder), one-sided Jacobi on X = R^H
+// (R^H = U_x S V_x^H, so Z = (Q V_x) S U_x^H). The columns of R^H start
+// closer to orthogonal than Z's, and the Jacobi iteration needs about half
+// the sweeps on the graded cores of the simple update. Same contract as
+// hestenes(Z, zr, zr, kk, V, kk, ...): on return column j of Z is s_j u_j (zero
+// for a numerically null s_j), V (kk x kk, ld kk) holds orthonormal right
+// singular vectors (null columns completed), s unsorted. V must have room for
+// zr x kk entries; X (kk x kk) and tau (kk) are scratch; acc (kk ints) is
+// overwritten. All in shared memory.
+static __device__ void hestenes_qr(cd *Z, int zr, int kk, cd *V, cd *X, cd *tau, double *s, int *flag, int *acc,
+                                   double *red) {
+  const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5;
+  householder_qr_owned(Z, zr, kk, tau);
+  for (int idx = tid; idx < kk * kk; idx += nt) {  // X = R^H
+    const int i = idx % kk, j = idx / kk;
+    X[idx] = j <= i ? cconj(Z[j + (long long)i * zr]) : czero();
+  }
+  __syncthreads();
+  hestenes(X, kk, kk, kk, V, kk, s, flag, red);  // X = U_x S, V = V_x
+  // V_x (ld kk) spread to ld zr with zero rows kk..zr-1, last column first (new
+  // positions lie at or after the old ones); one warp, kk <= 64 (two rows a lane)
+  if (warp == 0 && zr != kk) {
+    for (int j = kk - 1; j >= 0; --j) {
+      const cd v0 = lane < kk ? V[lane + (long long)j * kk] : czero();
+      const cd v1 = lane + 32 < kk ? V[lane + 32 + (long long)j * kk] : czero();
+      __syncwarp();
+      for (int i = lane; i < zr; i += 32) V[i + (long long)j * zr] = i < kk ? (i < 32 ? v0 : v1) : czero();
+      __syncwarp();
+    }
+  }
+  __syncthreads();
+  apply_q(Z, zr, kk, tau, V, zr, kk);  // V = Q [V_x; 0] = U_Z
+  for (int idx = tid; idx < zr * kk; idx += nt) Z[idx] = cscale(V[idx], s[idx / zr]);
+  __syncthreads();
+  for (int idx = tid; idx < kk * kk; idx += nt) {  // V = U_x (normalised columns of X)
+    const double sj = s[idx / kk];
+    V[idx] = sj > 0.0 ? cscale(X[idx], 1.0 / sj) : czero();
+  }
+  for (int j = tid; j < kk; j += nt) acc[j] = s[j] > 0.0 ? 1 : 0;
+  __syncthreads();
+  complete_orthonormal(V, kk, kk, kk, acc);
+}
+
 // ------------------------------------------------------------------ warp
 // Warp-synchronous forms for small matrices (n <= 32): one warp owns a
 // matrix in its own shared memory, so phases are separated by __syncwarp
@@ -527,9 +578,8 @@ static __device__ void warp_hestenes(cd *A, int lda, int m, int n, cd *V, int ld
               be += cabs2(y);
               cfmac(ga, x, y);
             }
-            double ag = sqrt(cabs2(ga));
             Rot rt;
-            if (al > null_thr && be > null_thr && ag > tol * sqrt(al) * sqrt(be) && jacobi_rot(al, be, ga, rt)) {
+            if (al > null_thr && be > null_thr && cabs2(ga) > tol * tol * al * be && jacobi_rot(al, be, ga, rt)) {
               rotated = true;
               for (int k = 0; k < m; ++k) {
                 cd x = ap[k], y = aq[k];

