@@ -117,23 +117,32 @@ class BPEngine:
         return "bp_node_k3" if self.layout.uniform_k3_chi() else "bp_node_generic"
 
     # -------------------------------------------------------------- load
+    def _load_pieces(self, arena: torch.Tensor, offsets, pieces: Sequence) -> None:
+        """Writes pieces (numpy or torch, any complex dtype) at the given
+        element offsets: host pieces are packed on the host and copied in one
+        transfer, device pieces are copied on the device."""
+        host = [p for p in pieces if not (isinstance(p, torch.Tensor) and p.is_cuda)]
+        if len(host) == len(pieces) and pieces:
+            buf = np.zeros(arena.numel(), dtype=np.complex128 if self.dtype == torch.complex128 else np.complex64)
+            for o, p in zip(offsets, pieces):
+                a = (p.numpy() if isinstance(p, torch.Tensor) else np.asarray(p)).reshape(-1)
+                buf[int(o) : int(o) + a.size] = a
+            arena.copy_(torch.from_numpy(buf))
+            return
+        for o, p in zip(offsets, pieces):
+            tt = p if isinstance(p, torch.Tensor) else torch.from_numpy(np.asarray(p))
+            arena[int(o) : int(o) + tt.numel()] = tt.reshape(-1).to(arena.device, self.dtype)
+
     def load_tensors(self, tensors_by_node: Sequence) -> None:
         """Node tensors in traversal node order (numpy or torch, any complex dtype)."""
-        L = self.layout
-        for v, t in enumerate(tensors_by_node):
-            tt = t if isinstance(t, torch.Tensor) else torch.from_numpy(np.asarray(t))
-            o = int(L.node_off[v])
-            self.T[o : o + tt.numel()] = tt.reshape(-1).to(L.device, self.dtype)
+        self._load_pieces(self.T, self.layout.node_off, list(tensors_by_node))
         self._bf16_stale = True
 
     def load_messages(self, n2e_by_half: Sequence, e2n_by_half: Optional[Sequence] = None) -> None:
         L = self.layout
         e2n_by_half = e2n_by_half if e2n_by_half is not None else n2e_by_half
         for arena, mats in ((self.n2e, n2e_by_half), (self.e2n, e2n_by_half)):
-            for h, m in enumerate(mats):
-                mm = m if isinstance(m, torch.Tensor) else torch.from_numpy(np.asarray(m))
-                o = int(L.half_msg_off[h])
-                arena[o : o + mm.numel()] = mm.reshape(-1).to(L.device, self.dtype)
+            self._load_pieces(arena, L.half_msg_off, list(mats))
 
     def _staged(self, src: torch.Tensor, dst: torch.Tensor) -> None:
         """Asynchronous H2D of a pinned host arena into ``dst``; a dtype
