@@ -370,14 +370,15 @@ def packed_inputs(g, tensors):
     return torch.from_numpy(np.ascontiguousarray(tensors[perm]).reshape(-1)).pin_memory()
 
 
-def convergence_study(seeds=(0, 1, 2), tol=1e-6, max_sweeps=400, bf16_tol=2e-4):
+def convergence_study(seeds=(0, 1, 2), tol=1e-6, max_sweeps=400, bf16_tol=1e-4, bf16_max_sweeps=60):
     """BP run to a message distance of ``tol`` from the same start in each
     form, then the Vidal gauge and the one-site densities (all FP64 on the
     final messages), for several seeds of the bench workload:
     * fp64: FP64 sweeps to ``tol``;
     * fp32: FP32 sweeps to ``tol``;
     * mixed: BF16 tensor-core sweeps to ``bf16_tol`` (above their rounding
-      floor of ~5e-5), then an FP32 refinement tail to ``tol``.
+      floor of ~5e-5; the distance read every second sweep, at most
+      ``bf16_max_sweeps``), then an FP32 refinement tail to ``tol``.
     Per form: sweeps, device time to the tolerance (CUDA events around the
     loop, distance read back every sweep), and against FP64 the largest
     |delta lambda| over all bond spectra, the largest |delta rho_i| entry over
@@ -428,7 +429,7 @@ def convergence_study(seeds=(0, 1, 2), tol=1e-6, max_sweeps=400, bf16_tol=2e-4):
         etail = engine(g, "fp32", packed, m)
 
         def mixed():
-            nb = ebf.run(bf16_tol, max_sweeps)
+            nb = ebf.run(bf16_tol, bf16_max_sweeps, check_every=2)
             etail.n2e.copy_(ebf.n2e)
             etail.e2n.copy_(ebf.e2n)
             nt = etail.run(tol, max_sweeps)
