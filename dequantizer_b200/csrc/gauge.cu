@@ -29,9 +29,19 @@ __device__ __forceinline__ double safe_truncate(double l, double eps) { return l
 
 // ----------------------------------------------------------- vidal edges
 // Work buffers per edge (each chi^2 complex): Af Vf Ab Vb Qf Qb C W, plus
-// wf wb s (chi doubles each), perm/acc ints.
+// wf wb s wif wib (chi doubles each), perm/acc ints.
 __host__ __device__ inline size_t vidal_edge_bytes(int c) {
-  return 8 * (size_t)c * c * sizeof(cd) + 3 * (size_t)c * sizeof(double) + 2 * (size_t)c * sizeof(int) + 64;
+  return 8 * (size_t)c * c * sizeof(cd) + 5 * (size_t)c * sizeof(double) + 2 * (size_t)c * sizeof(int) + 64;
+}
+
+// The eigenvalue weights of sqrt(m) and its safe inverse, once per eigenvalue
+// (not per matrix element): w <- sqrt(safe_truncate(w)), wi <- sqrt(safe_inverse(w)).
+__device__ __forceinline__ void sqrt_weights(double *w, double *wi, int c, double eps, int i0, int step) {
+  for (int k = i0; k < c; k += step) {
+    const double l = w[k];
+    wi[k] = sqrt(safe_inverse(l, eps));
+    w[k] = sqrt(safe_truncate(l, eps));
+  }
 }
 
 __host__ __device__ inline size_t round16(size_t x) { return (x + 15) & ~(size_t)15; }
@@ -50,8 +60,8 @@ __global__ void __launch_bounds__(GAUGE_THREADS) vidal_edges_kernel(dqz_graph_t 
   cd *Af = reinterpret_cast<cd *>(base);
   cd *Vf = Af + M2, *Ab = Vf + M2, *Vb = Ab + M2, *Qf = Vb + M2, *Qb = Qf + M2, *C = Qb + M2, *W = C + M2;
   double *wf = reinterpret_cast<double *>(W + M2);
-  double *wb = wf + max_chi, *sv = wb + max_chi;
-  int *perm = reinterpret_cast<int *>(sv + max_chi);
+  double *wb = wf + max_chi, *sv = wb + max_chi, *wif = sv + max_chi, *wib = wif + max_chi;
+  int *perm = reinterpret_cast<int *>(wib + max_chi);
   const int tid = threadIdx.x, nt = blockDim.x;
 
   const int total = sel ? n_sel : g.n_edges;
@@ -68,6 +78,9 @@ __global__ void __launch_bounds__(GAUGE_THREADS) vidal_edges_kernel(dqz_graph_t 
     __syncthreads();
     herm_eigh(Af, c, Vf, c, c, wf, rots, red);
     herm_eigh(Ab, c, Vb, c, c, wb, rots, red);
+    sqrt_weights(wf, wif, c, eps, tid, nt);
+    sqrt_weights(wb, wib, c, eps, tid, nt);
+    __syncthreads();
     // Af <- sqrt(m_f), Qf <- sqrt(m_f)^+ (safe), same for b.
     for (int idx = tid; idx < c * c; idx += nt) {
       const int i = idx / c, j = idx % c;
@@ -75,10 +88,10 @@ __global__ void __launch_bounds__(GAUGE_THREADS) vidal_edges_kernel(dqz_graph_t 
       for (int k = 0; k < c; ++k) {
         cd pf = cmul(Vf[i * c + k], cconj(Vf[j * c + k]));
         cd pb = cmul(Vb[i * c + k], cconj(Vb[j * c + k]));
-        sf = cadd(sf, cscale(pf, sqrt(safe_truncate(wf[k], eps))));
-        sif = cadd(sif, cscale(pf, sqrt(safe_inverse(wf[k], eps))));
-        sb = cadd(sb, cscale(pb, sqrt(safe_truncate(wb[k], eps))));
-        sib = cadd(sib, cscale(pb, sqrt(safe_inverse(wb[k], eps))));
+        sf = cadd(sf, cscale(pf, wf[k]));
+        sif = cadd(sif, cscale(pf, wif[k]));
+        sb = cadd(sb, cscale(pb, wb[k]));
+        sib = cadd(sib, cscale(pb, wib[k]));
       }
       Af[idx] = sf;
       Qf[idx] = sif;
@@ -155,8 +168,8 @@ __global__ void __launch_bounds__(GAUGE_THREADS) vidal_edges_warp_kernel(dqz_gra
   cd *Af = reinterpret_cast<cd *>(base);
   cd *Vf = Af + M2, *Ab = Vf + M2, *Vb = Ab + M2, *Qf = Vb + M2, *Qb = Qf + M2, *C = Qb + M2, *W = C + M2;
   double *wf = reinterpret_cast<double *>(W + M2);
-  double *wb = wf + max_chi, *sv = wb + max_chi;
-  int *perm = reinterpret_cast<int *>(sv + max_chi);
+  double *wb = wf + max_chi, *sv = wb + max_chi, *wif = sv + max_chi, *wib = wif + max_chi;
+  int *perm = reinterpret_cast<int *>(wib + max_chi);
   const int total = sel ? n_sel : g.n_edges;
   for (int it = blockIdx.x * wpb + wid; it < total; it += gridDim.x * wpb) {
     const int e = sel ? sel[it] : it;
@@ -176,16 +189,19 @@ __global__ void __launch_bounds__(GAUGE_THREADS) vidal_edges_warp_kernel(dqz_gra
     __syncwarp();
     warp_herm_eigh(Af, c, Vf, c, c, wf, rots);
     warp_herm_eigh(Ab, c, Vb, c, c, wb, rots);
+    sqrt_weights(wf, wif, c, eps, lane, 32);
+    sqrt_weights(wb, wib, c, eps, lane, 32);
+    __syncwarp();
     for (int idx = lane; idx < c * c; idx += 32) {
       const int i = idx / c, j = idx % c;
       cd sf = czero(), sif = czero(), sb = czero(), sib = czero();
       for (int k = 0; k < c; ++k) {
         cd pf = cmul(Vf[i * c + k], cconj(Vf[j * c + k]));
         cd pb = cmul(Vb[i * c + k], cconj(Vb[j * c + k]));
-        sf = cadd(sf, cscale(pf, sqrt(safe_truncate(wf[k], eps))));
-        sif = cadd(sif, cscale(pf, sqrt(safe_inverse(wf[k], eps))));
-        sb = cadd(sb, cscale(pb, sqrt(safe_truncate(wb[k], eps))));
-        sib = cadd(sib, cscale(pb, sqrt(safe_inverse(wb[k], eps))));
+        sf = cadd(sf, cscale(pf, wf[k]));
+        sif = cadd(sif, cscale(pf, wif[k]));
+        sb = cadd(sb, cscale(pb, wb[k]));
+        sib = cadd(sib, cscale(pb, wib[k]));
       }
       Af[idx] = sf;
       Qf[idx] = sif;
