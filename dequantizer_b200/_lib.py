@@ -84,7 +84,6 @@ _SIGNATURES = {
     "dqz_bp_edge_pass_c64": (ctypes.c_int, [_G, _P, _P, _P, _P, _P]),
     "dqz_bp_node_update_k3_tc": (ctypes.c_int, [_G, _P, _P, _P, _P, _P, _P, _I, _P, _P]),
     "dqz_bp_node_update_k3_umma": (ctypes.c_int, [_G, _P, _P, _P, _P, _P, _P, _I, _P, _P]),
-    "dqz_bp_sweep_k3_umma": (ctypes.c_int, [_G, _P, _P, _P, _P, _P, _P, _P, _I, _P, _P]),
     "dqz_bf16_umma_elems_per_node": (_S, []),
     "dqz_pack_bf16_umma": (ctypes.c_int, [_G, _P, _P, _P]),
     "dqz_pack_bf16_umma_nodes": (ctypes.c_int, [_G, _P, _P, _I, _I, _P]),

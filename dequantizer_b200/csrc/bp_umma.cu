@@ -90,7 +90,6 @@ struct NodeMeta {
   int off[3];   // half_msg_off of the node's half-edges (where its messages go)
   int src[3];   // source arena of each incoming message: 0 e2n_old, 1 n2e_old, 2 n2e_new
   int moff[3];  // element offset of each incoming message in that arena
-  int toff[3];  // half_msg_off of the twin half-edges (the fused edge pass reads n2e_old there)
 };
 struct MetaChain {  // intermediate levels of the next node's metadata
   int v, vn, h0, deg, phys;  // vn: the node after it
@@ -213,8 +212,8 @@ __device__ __forceinline__ uint32_t frag_addr(const __nv_bfloat16 *base, Core co
 
 __global__ void __launch_bounds__(UM_THREADS, 2)
     bp_node_k3_umma(dqz_graph_t g, const __nv_bfloat16 *__restrict__ Tu, const float2 *n2e_old, const float2 *e2n_old,
-                    float2 *n2e_new, float2 *e2n_new, const uint8_t *__restrict__ src_sel,
-                    const int32_t *__restrict__ nodes, int n_nodes, int *error_flag) {
+                    float2 *n2e_new, const uint8_t *__restrict__ src_sel, const int32_t *__restrict__ nodes,
+                    int n_nodes, int *error_flag) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   UmSmem &S = *reinterpret_cast<UmSmem *>(smem_raw);
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5, wq = w & 3;
@@ -298,7 +297,6 @@ __global__ void __launch_bounds__(UM_THREADS, 2)
       M.off[q] = S.chain.hoff[q];
       M.src[q] = sel == DQZ_SRC_E2N_OLD ? 0 : (sel == DQZ_SRC_N2E_NEW ? 2 : 1);
       M.moff[q] = sel == DQZ_SRC_E2N_OLD ? S.chain.hoff[q] : (ok ? (int)g.half_msg_off[tw] : 0);
-      M.toff[q] = ok ? (int)g.half_msg_off[tw] : 0;
     }
     M.v = S.chain.v;
     M.ok = ok;
@@ -366,12 +364,6 @@ __global__ void __launch_bounds__(UM_THREADS, 2)
       if (has_next) prepare_blocking(next, cur ^ 1);
       cur ^= 1;
       continue;
-    }
-    if (e2n_new) {  // fused edge pass of the synchronous sweep: e2n_new[h] = n2e_old[twin(h)] for this
-                    // node's half-edges, while the slice copies are still landing
-      const NodeMeta &Mc = S.meta[cur];
-#pragma unroll
-      for (int e = 0; e < 3; ++e) e2n_new[Mc.off[e] + tid] = n2e_old[Mc.toff[e] + tid];
     }
     float fr[3][2][4] = {}, fi[3][2][4] = {};  // this warp's partial final products
     float2 xn[3];                               // next node's message elements
@@ -588,7 +580,6 @@ __global__ void __launch_bounds__(UM_THREADS, 2)
       __syncthreads();
 #pragma unroll
       for (int e = 0; e < 3; ++e) n2e_new[S.meta[cur].off[e] + tid] = out_s[e * 256 + (tid ^ (tid >> 4))];
-
     }
     cur ^= 1;
   }
@@ -662,33 +653,10 @@ extern "C" int dqz_pack_bf16_umma_nodes(const dqz_graph_t *g, const void *tensor
   return DQZ_OK;
 }
 
-namespace {
-int launch_umma(const dqz_graph_t *g, const void *tensors_bf16, const void *n2e_old, const void *e2n_old,
-                void *n2e_new, void *e2n_new, const uint8_t *src_sel, const int32_t *nodes, int32_t n_nodes,
-                int32_t *error_flag, cudaStream_t stream);
-}
-
 extern "C" int dqz_bp_node_update_k3_umma(const dqz_graph_t *g, const void *tensors_bf16, const void *n2e_old,
                                           const void *e2n_old, void *n2e_new, const uint8_t *src_sel,
                                           const int32_t *nodes, int32_t n_nodes, int32_t *error_flag,
                                           cudaStream_t stream) {
-  return launch_umma(g, tensors_bf16, n2e_old, e2n_old, n2e_new, nullptr, src_sel, nodes, n_nodes, error_flag,
-                     stream);
-}
-
-extern "C" int dqz_bp_sweep_k3_umma(const dqz_graph_t *g, const void *tensors_bf16, const void *n2e_old,
-                                    const void *e2n_old, void *n2e_new, void *e2n_new, const uint8_t *src_sel,
-                                    const int32_t *nodes, int32_t n_nodes, int32_t *error_flag,
-                                    cudaStream_t stream) {
-  if (!e2n_new) return DQZ_ERR_ARG;
-  return launch_umma(g, tensors_bf16, n2e_old, e2n_old, n2e_new, e2n_new, src_sel, nodes, n_nodes, error_flag,
-                     stream);
-}
-
-namespace {
-int launch_umma(const dqz_graph_t *g, const void *tensors_bf16, const void *n2e_old, const void *e2n_old,
-                void *n2e_new, void *e2n_new, const uint8_t *src_sel, const int32_t *nodes, int32_t n_nodes,
-                int32_t *error_flag, cudaStream_t stream) {
   if (!g || !tensors_bf16 || !n2e_old || !e2n_old || !n2e_new || !src_sel || !nodes || !error_flag || n_nodes < 0)
     return DQZ_ERR_ARG;
   if (((uintptr_t)tensors_bf16 & 15) != 0) return DQZ_ERR_ARG;  // bulk copies start on 16-byte boundaries
@@ -707,9 +675,7 @@ int launch_umma(const dqz_graph_t *g, const void *tensors_bf16, const void *n2e_
   const int grid = n_nodes < 2 * sms ? n_nodes : 2 * sms;
   bp_node_k3_umma<<<grid, UM_THREADS, smem, stream>>>(*g, (const __nv_bfloat16 *)tensors_bf16,
                                                       (const float2 *)n2e_old, (const float2 *)e2n_old,
-                                                      (float2 *)n2e_new, (float2 *)e2n_new, src_sel, nodes, n_nodes,
-                                                      error_flag);
+                                                      (float2 *)n2e_new, src_sel, nodes, n_nodes, error_flag);
   DQZ_CHECK_LAUNCH();
   return DQZ_OK;
 }
-}  // namespace

@@ -34,8 +34,7 @@ import torch
 from . import _lib
 from .graph import TensorGraph
 from .layout import GraphLayout
-from .maps import (BF16_KERNELS, Topology, bp_sweep, density_packed, error_flag, fused_edge_pass, vidal_distance_packed,
-                   vidal_gauge_packed)
+from .maps import BF16_KERNELS, Topology, bp_sweep, density_packed, error_flag, vidal_distance_packed, vidal_gauge_packed
 
 log = logging.getLogger(__name__)
 
@@ -209,7 +208,6 @@ class BPEngine:
         src_sel, edge_new, _ = topo.device_tables(L.device)
         n2e_new, e2n_new = self._spare
         chi = L.uniform_k3_chi()
-        fused = self.T_bf16 is not None and fused_edge_pass(topo)
         flag = error_flag(L.device)
         stream = _lib.stream_handle()
 
@@ -246,14 +244,9 @@ class BPEngine:
             if self.T_bf16 is not None:
                 _lib.call("dqz_pack_bf16_umma_nodes", L.gptr, self.T.data_ptr(), self.T_bf16.data_ptr(), lo, hi - lo,
                           stream)
-                if fused:  # this range's edge pass inside its node update
-                    _lib.call("dqz_bp_sweep_k3_umma", L.gptr, self.T_bf16.data_ptr(), self.n2e.data_ptr(),
-                              self.e2n.data_ptr(), n2e_new.data_ptr(), e2n_new.data_ptr(), src_sel.data_ptr(),
-                              ids.data_ptr(), ids.numel(), flag.data_ptr(), stream)
-                else:
-                    _lib.call(BF16_KERNELS["tcgen05"], L.gptr, self.T_bf16.data_ptr(), self.n2e.data_ptr(),
-                              self.e2n.data_ptr(), n2e_new.data_ptr(), src_sel.data_ptr(), ids.data_ptr(),
-                              ids.numel(), flag.data_ptr(), stream)
+                _lib.call(BF16_KERNELS["tcgen05"], L.gptr, self.T_bf16.data_ptr(), self.n2e.data_ptr(),
+                          self.e2n.data_ptr(), n2e_new.data_ptr(), src_sel.data_ptr(), ids.data_ptr(), ids.numel(),
+                          flag.data_ptr(), stream)
             else:
                 _lib.call("dqz_bp_node_update_k3", L.gptr, chi, 64 if self.T.dtype == torch.complex128 else 32,
                           self.T.data_ptr(), self.n2e.data_ptr(), self.e2n.data_ptr(), n2e_new.data_ptr(),
@@ -261,9 +254,7 @@ class BPEngine:
             down.wait_event(cur.record_event())
             with torch.cuda.stream(down):
                 out_n2e[ma:mb].copy_(n2e_new[ma:mb], non_blocking=True)
-        if fused:
-            pass
-        elif self.T.dtype == torch.complex64:
+        if self.T.dtype == torch.complex64:
             _lib.call("dqz_bp_edge_pass_c64", L.gptr, self.n2e.data_ptr(), n2e_new.data_ptr(), edge_new.data_ptr(),
                       e2n_new.data_ptr(), stream)
         else:
@@ -295,8 +286,6 @@ class BPEngine:
         self.n2e, self.e2n = n2e_new, e2n_new
 
     def launches_per_sweep(self) -> int:
-        if self.T_bf16 is not None and self.bf16_kernel == "tcgen05" and fused_edge_pass(self.topo):
-            return 1  # the edge pass runs inside the tcgen05 node update (dqz_bp_sweep_k3_umma)
         if len(self.topo.levels) > 1 and self.T.dtype == torch.complex128 and not self.layout.uniform_k3_chi():
             return 1  # every level and the edge pass in one cooperative launch (dqz_bp_sweep_levels)
         return len(self.topo.levels) + 1

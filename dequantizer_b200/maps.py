@@ -189,13 +189,6 @@ def error_flag(device) -> torch.Tensor:
 BF16_KERNELS = {"tcgen05": "dqz_bp_node_update_k3_umma", "mma_sync": "dqz_bp_node_update_k3_tc"}
 
 
-def fused_edge_pass(topo: Topology) -> bool:
-    """Whether a sweep's edge pass can run inside its node update: one node
-    level and every edge forwarding the old node->edge messages (the
-    reference's synchronous schedule)."""
-    return len(topo.levels) == 1 and topo.is_synchronous and not topo.flooding and not topo.edge_new.any()
-
-
 def bp_sweep(layout: GraphLayout, topo: Topology, T, n2e_old, e2n_old, n2e_new, e2n_new, mid_event=None,
              T_bf16=None, bf16_kernel: str = "tcgen05"):
     """One sweep on packed arenas: node updates level by level, then the edge pass
@@ -215,15 +208,6 @@ def bp_sweep(layout: GraphLayout, topo: Topology, T, n2e_old, e2n_old, n2e_new, 
             raise NotImplementedError("complex64 BP needs degree-3 nodes with bonds of dimension 8 or 16 "
                                       "(16 for the tensor-core form)")
         flag = error_flag(layout.device)
-        if T_bf16 is not None and bf16_kernel == "tcgen05" and fused_edge_pass(topo):
-            # the reference's synchronous sweep: one launch, the edge pass fused into the node update
-            nodes = topo.device_node_levels(layout.device)[0]
-            _lib.call("dqz_bp_sweep_k3_umma", layout.gptr, T_bf16.data_ptr(), n2e_old.data_ptr(), e2n_old.data_ptr(),
-                      n2e_new.data_ptr(), e2n_new.data_ptr(), src_sel.data_ptr(), nodes.data_ptr(), nodes.numel(),
-                      flag.data_ptr(), stream)
-            if mid_event is not None:
-                mid_event.record(torch.cuda.current_stream())
-            return
         if T_bf16 is not None:
             for nodes in topo.device_node_levels(layout.device):
                 _lib.call(BF16_KERNELS[bf16_kernel], layout.gptr, T_bf16.data_ptr(), n2e_old.data_ptr(),

@@ -136,15 +136,6 @@ int dqz_bp_node_update_k3_umma(const dqz_graph_t *g, const void *tensors_bf16, c
                                const int32_t *nodes, int32_t n_nodes, int32_t *error_flag,
                                cudaStream_t stream);
 size_t dqz_bf16_umma_elems_per_node(void);
-/* The same node update with the edge pass of the reference's synchronous
- * sweep fused in (tensor_ops.py:70-76, mappings/belief_propagation.py:38):
- * each CTA also writes e2n_new[h] = n2e_old[twin(h)] for its node's
- * half-edges, so a synchronous sweep over every node is one launch. For
- * schedules whose edges read the old node->edge messages (src_sel all
- * DQZ_SRC_E2N_OLD); e2n_new is written for the listed nodes' half-edges only. */
-int dqz_bp_sweep_k3_umma(const dqz_graph_t *g, const void *tensors_bf16, const void *n2e_old,
-                         const void *e2n_old, void *n2e_new, void *e2n_new, const uint8_t *src_sel,
-                         const int32_t *nodes, int32_t n_nodes, int32_t *error_flag, cudaStream_t stream);
 /* complex64 node tensors (node_off layout) -> the BF16 core layouts above. */
 int dqz_pack_bf16_umma(const dqz_graph_t *g, const void *tensors_c64, void *tensors_bf16,
                        cudaStream_t stream);
