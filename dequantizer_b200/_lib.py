@@ -80,6 +80,8 @@ _SIGNATURES = {
     "dqz_bp_node_scratch_bytes": (_S, [_I, _I, _I]),
     "dqz_bp_edge_pass": (ctypes.c_int, [_G, _P, _P, _P, _P, _I, _P]),
     "dqz_bp_sweep_levels": (ctypes.c_int, [_G, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I, _I, _I, _I, _P, _P, _P]),
+    "dqz_bp_sweep_sliced": (ctypes.c_int, [_G, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I, _I, _I, _I, _P, _P,
+                                           _P]),
     "dqz_bp_node_update_k3": (ctypes.c_int, [_G, _I, _I, _P, _P, _P, _P, _P, _P, _I, _P, _P]),
     "dqz_bp_edge_pass_c64": (ctypes.c_int, [_G, _P, _P, _P, _P, _P]),
     "dqz_bp_node_update_k3_tc": (ctypes.c_int, [_G, _P, _P, _P, _P, _P, _P, _I, _P, _P]),

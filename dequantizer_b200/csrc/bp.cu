@@ -29,6 +29,64 @@ __device__ __forceinline__ const cd *incoming_msg(const dqz_graph_t &g, int hf, 
   return (sel == DQZ_SRC_N2E_NEW ? n2e_new : n2e_old) + g.half_msg_off[tw];
 }
 
+// Column a of the unnormalised outgoing message of bond e of a node (tensor
+// Tv, shape s): out[ap][a] = sum_x conj(T_slice(ap)[x]) Y_a[x], with Y_a the
+// bond-e slice a contracted with the k-1 incoming messages; `put(ap, value)`
+// stores each entry. bufA / bufB hold two slices. Whole CTA; ends with a barrier.
+template <typename Put>
+__device__ __forceinline__ void node_slice_column(const dqz_graph_t &g, const cd *__restrict__ Tv, const NodeShape &s,
+                                                  int e, const cd *n2e_old, const cd *e2n_old, const cd *n2e_new,
+                                                  const uint8_t *__restrict__ src_sel, int a, cd *bufA, cd *bufB,
+                                                  Put put) {
+  const int ce = s.dims[e];
+  const long long Re = s.stride[e];
+  const long long P = s.size / ce;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (long long x = threadIdx.x; x < P; x += blockDim.x) {
+    long long l = x / Re, r = x - l * Re;
+    bufA[x] = Tv[(l * ce + a) * Re + r];
+  }
+  __syncthreads();
+  cd *cur = bufA, *nxt = bufB;
+  long long Lj = 1;
+  for (int f = 0; f < s.k; ++f) {
+    if (f == e) continue;
+    const int q = s.dims[f];
+    const long long R = P / Lj / q;
+    const cd *m = incoming_msg(g, s.half0 + f, n2e_old, e2n_old, n2e_new, src_sel);
+    mode_product<false>(cur, nxt, Lj, q, q, R, m, q, 1);
+    __syncthreads();
+    cd *t = cur;
+    cur = nxt;
+    nxt = t;
+    Lj *= q;
+  }
+  for (int ap = warp; ap < ce; ap += nw) {
+    cd acc = czero();
+    for (long long x = lane; x < P; x += 32) {
+      long long l = x / Re, r = x - l * Re;
+      cfmac(acc, Tv[(l * ce + ap) * Re + r], cur[x]);
+    }
+    acc = warp_csum(acc);
+    if (lane == 0) put(ap, acc);
+  }
+  __syncthreads();
+}
+
+// dst (ce x ce) /= its trace, the trace summed by one thread in index order.
+// Whole CTA; src may equal dst.
+__device__ __forceinline__ void normalise_by_trace(const cd *src, cd *dst, int ce, cd &trace_sh) {
+  if (threadIdx.x == 0) {
+    cd tr = czero();
+    for (int i = 0; i < ce; ++i) tr = cadd(tr, src[i * ce + i]);
+    trace_sh = tr;
+  }
+  __syncthreads();
+  const cd tr = trace_sh;
+  for (int i = threadIdx.x; i < ce * ce; i += blockDim.x) dst[i] = cdiv(src[i], tr);
+  __syncthreads();
+}
+
 // n2e_new[h] for one half-edge h by the whole CTA (out: ce x ce, bufA / bufB:
 // two slices, trace_sh: one shared complex). Ends with a barrier.
 __device__ __forceinline__ void node_update_half(const dqz_graph_t &g, const cd *__restrict__ T, const cd *n2e_old,
@@ -40,51 +98,10 @@ __device__ __forceinline__ void node_update_half(const dqz_graph_t &g, const cd 
   const int e = h - s.half0;
   const int ce = s.dims[e];
   const cd *Tv = T + g.node_off[v];
-  const long long Re = s.stride[e];
-  const long long P = s.size / ce;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-
-  for (int a = 0; a < ce; ++a) {
-    for (long long x = threadIdx.x; x < P; x += blockDim.x) {
-      long long l = x / Re, r = x - l * Re;
-      bufA[x] = Tv[(l * ce + a) * Re + r];
-    }
-    __syncthreads();
-    cd *cur = bufA, *nxt = bufB;
-    long long Lj = 1;
-    for (int f = 0; f < s.k; ++f) {
-      if (f == e) continue;
-      const int q = s.dims[f];
-      const long long R = P / Lj / q;
-      const cd *m = incoming_msg(g, s.half0 + f, n2e_old, e2n_old, n2e_new, src_sel);
-      mode_product<false>(cur, nxt, Lj, q, q, R, m, q, 1);
-      __syncthreads();
-      cd *t = cur;
-      cur = nxt;
-      nxt = t;
-      Lj *= q;
-    }
-    for (int ap = warp; ap < ce; ap += nw) {
-      cd acc = czero();
-      for (long long x = lane; x < P; x += 32) {
-        long long l = x / Re, r = x - l * Re;
-        cfmac(acc, Tv[(l * ce + ap) * Re + r], cur[x]);
-      }
-      acc = warp_csum(acc);
-      if (lane == 0) out[ap * ce + a] = acc;
-    }
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) {
-    cd tr = czero();
-    for (int i = 0; i < ce; ++i) tr = cadd(tr, out[i * ce + i]);
-    trace_sh = tr;
-  }
-  __syncthreads();
-  const cd tr = trace_sh;
-  cd *dst = n2e_new + g.half_msg_off[h];
-  for (int i = threadIdx.x; i < ce * ce; i += blockDim.x) dst[i] = cdiv(out[i], tr);
-  __syncthreads();
+  for (int a = 0; a < ce; ++a)
+    node_slice_column(g, Tv, s, e, n2e_old, e2n_old, n2e_new, src_sel, a, bufA, bufB,
+                      [&](int ap, cd val) { out[ap * ce + a] = val; });
+  normalise_by_trace(out, n2e_new + g.half_msg_off[h], ce, trace_sh);
 }
 
 __global__ void __launch_bounds__(BP_THREADS) bp_node_generic(dqz_graph_t g, const cd *__restrict__ T,
@@ -161,6 +178,56 @@ __global__ void __launch_bounds__(BP_THREADS) bp_sweep_levels_kernel(
     if (!grid_barrier(sync, gen, error_flag)) return;
   }
   // edge pass: e2n_new[h] = (edge_new[h] ? n2e_new : n2e_old)[twin(h)], one warp per half-edge
+  const int wpb = blockDim.x >> 5;
+  for (int h = blockIdx.x * wpb + (threadIdx.x >> 5); h < g.n_halves; h += gridDim.x * wpb) {
+    const int e = g.half_edge[h];
+    const int tw = g.half_twin[h];
+    if (e < 0 || tw < 0) continue;
+    const int c = g.edge_chi[e];
+    const cd *src = (edge_new[h] ? n2e_new : n2e_old) + g.half_msg_off[tw];
+    cd *dst = e2n_new + g.half_msg_off[h];
+    warp_copy16(reinterpret_cast<uint4 *>(dst), reinterpret_cast<const uint4 *>(src), c * c);
+  }
+}
+
+// The same sweep with each half-edge's slices spread over the grid (for
+// large bonds, where a level has few half-edges but each carries much work):
+// per level, every (half-edge, slice) item writes its unnormalised column of
+// the outgoing message; after a grid barrier each half-edge of the level is
+// divided by its trace; a second barrier closes the level. Same arithmetic and
+// order as bp_node_generic, so the messages are bit-identical.
+__global__ void __launch_bounds__(BP_THREADS) bp_sweep_sliced_kernel(
+    dqz_graph_t g, const cd *__restrict__ T, const cd *n2e_old, const cd *e2n_old, cd *n2e_new, cd *e2n_new,
+    const uint8_t *__restrict__ src_sel, const uint8_t *__restrict__ edge_new, const int32_t *__restrict__ halves,
+    const int32_t *__restrict__ level_off, const int32_t *__restrict__ item_half,
+    const int32_t *__restrict__ item_slice, const int32_t *__restrict__ item_off, int n_levels, int max_slice,
+    int max_chi, unsigned *sync, int *error_flag) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cd *bufA = reinterpret_cast<cd *>(smem_raw + 48 * sizeof(double)) + (long long)max_chi * max_chi;
+  cd *bufB = bufA + max_slice;
+  __shared__ cd trace_sh;
+  unsigned gen = 0;
+  for (int lv = 0; lv < n_levels; ++lv) {
+    for (int item = item_off[lv] + blockIdx.x; item < item_off[lv + 1]; item += gridDim.x) {
+      const int h = item_half[item], a = item_slice[item];
+      const int v = g.half_node[h];
+      NodeShape s;
+      load_shape(g, v, s);
+      const int e = h - s.half0;
+      const int ce = s.dims[e];
+      cd *dst = n2e_new + g.half_msg_off[h];
+      node_slice_column(g, T + g.node_off[v], s, e, n2e_old, e2n_old, n2e_new, src_sel, a, bufA, bufB,
+                        [&](int ap, cd val) { dst[ap * ce + a] = val; });
+    }
+    if (!grid_barrier(sync, gen, error_flag)) return;
+    for (int i = level_off[lv] + blockIdx.x; i < level_off[lv + 1]; i += gridDim.x) {
+      const int h = halves[i];
+      const int ce = g.edge_chi[g.half_edge[h]];
+      cd *m = n2e_new + g.half_msg_off[h];
+      normalise_by_trace(m, m, ce, trace_sh);
+    }
+    if (!grid_barrier(sync, gen, error_flag)) return;
+  }
   const int wpb = blockDim.x >> 5;
   for (int h = blockIdx.x * wpb + (threadIdx.x >> 5); h < g.n_halves; h += gridDim.x * wpb) {
     const int e = g.half_edge[h];
@@ -368,5 +435,47 @@ extern "C" int dqz_message_changes_c64(const dqz_graph_t *g, const void *n2e_a, 
   msg_dist_c64_kernel<<<(nh + wpb - 1) / wpb, wpb * 32, 0, stream>>>(*g, (const float2 *)n2e_a, (const float2 *)n2e_b,
                                                                    partial);
   DQZ_CHECK_LAUNCH();
+  return DQZ_OK;
+}
+
+extern "C" int dqz_bp_sweep_sliced(const dqz_graph_t *g, const void *tensors, const void *n2e_old,
+                                   const void *e2n_old, void *n2e_new, void *e2n_new, const uint8_t *src_sel,
+                                   const uint8_t *edge_new, const int32_t *halves, const int32_t *level_off,
+                                   const int32_t *item_half, const int32_t *item_slice, const int32_t *item_off,
+                                   int32_t n_levels, int32_t max_items, int32_t max_slice, int32_t max_chi,
+                                   uint32_t *sync, int32_t *error_flag, cudaStream_t stream) {
+  if (!g || !tensors || !n2e_old || !e2n_old || !n2e_new || !e2n_new || !src_sel || !edge_new || !halves ||
+      !level_off || !item_half || !item_slice || !item_off || !sync || !error_flag || n_levels <= 0 ||
+      max_items <= 0 || max_slice <= 0)
+    return DQZ_ERR_ARG;
+  if (max_chi <= 0 || max_chi > DQZ_MAX_CHI) return DQZ_ERR_UNSUPPORTED;
+  const size_t smem = bp_smem_bytes(max_slice, max_chi, false);
+  if (smem > BP_SMEM_LIMIT) return DQZ_ERR_UNSUPPORTED;
+  DQZ_SMEM_ATTR_ONCE(bp_sweep_sliced_kernel, BP_SMEM_LIMIT);
+  int dev = 0, sms = 148, per_sm = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return DQZ_ERR_CUDA;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bp_sweep_sliced_kernel, BP_THREADS, smem) !=
+          cudaSuccess ||
+      per_sm < 1)
+    return DQZ_ERR_UNSUPPORTED;
+  int grid = max_items;  // all co-resident
+  if (grid > sms * per_sm) grid = sms * per_sm;
+  if (cudaMemsetAsync(sync, 0, 2 * sizeof(uint32_t), stream) != cudaSuccess) return DQZ_ERR_CUDA;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(BP_THREADS);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  if (cudaLaunchKernelEx(&cfg, bp_sweep_sliced_kernel, *g, (const cd *)tensors, (const cd *)n2e_old,
+                         (const cd *)e2n_old, (cd *)n2e_new, (cd *)e2n_new, src_sel, edge_new, halves, level_off,
+                         item_half, item_slice, item_off, (int)n_levels, (int)max_slice, (int)max_chi,
+                         (unsigned *)sync, (int *)error_flag) != cudaSuccess)
+    return DQZ_ERR_CUDA;
   return DQZ_OK;
 }

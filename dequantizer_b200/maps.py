@@ -150,6 +150,30 @@ class Topology:
                               torch.zeros(2, dtype=torch.int32, device=device))
         return self._dev_flat
 
+    def device_slice_items(self, layout, device):
+        """The (half-edge, slice) work items of every level for the sliced
+        one-launch sweep (dqz_bp_sweep_sliced), from the layout's current bond
+        dimensions: item_half, item_slice, per-level offsets, the largest level."""
+        key = layout.edge_chi.tobytes()
+        cache = self.__dict__.setdefault("_dev_items", {})
+        if key not in cache:
+            he = layout.half_edge
+            ce = np.where(he >= 0, layout.edge_chi[np.maximum(he, 0)], 0).astype(np.int64)
+            halves, slices, off = [], [], [0]
+            for lv in self.levels:
+                c = ce[lv]
+                halves.append(np.repeat(lv, c))
+                slices.append(np.concatenate([np.arange(x) for x in c]) if len(c) else np.zeros(0, np.int64))
+                off.append(off[-1] + int(c.sum()))
+            ih = np.concatenate(halves).astype(np.int32)
+            isl = np.concatenate(slices).astype(np.int32)
+            widest = int(np.max(np.diff(off))) if len(off) > 1 else 0
+            if len(cache) > 8:
+                cache.clear()
+            cache[key] = (torch.from_numpy(ih).to(device), torch.from_numpy(isl).to(device),
+                          torch.from_numpy(np.array(off, dtype=np.int32)).to(device), widest)
+        return cache[key]
+
     def device_node_levels(self, device):
         if self._dev_nodes is None:
             self._dev_nodes = [torch.from_numpy(l).to(device) for l in self.node_levels]
@@ -187,6 +211,11 @@ def error_flag(device) -> torch.Tensor:
 
 
 BF16_KERNELS = {"tcgen05": "dqz_bp_node_update_k3_umma", "mma_sync": "dqz_bp_node_update_k3_tc"}
+
+# bonds from which the one-launch asynchronous sweep spreads slices (not whole
+# half-edges) over the grid: at bond 32 a level of the heavy-hex DFS schedule
+# has a handful of half-edges of ~50 MFLOP each
+SLICED_MIN_CHI = 8
 
 
 def bp_sweep(layout: GraphLayout, topo: Topology, T, n2e_old, e2n_old, n2e_new, e2n_new, mid_event=None,
@@ -239,10 +268,21 @@ def bp_sweep(layout: GraphLayout, topo: Topology, T, n2e_old, e2n_old, n2e_new, 
         # a schedule of several node levels (the reference's asynchronous sweep):
         # all levels and the edge pass in one launch when a slice fits on chip
         flat, off, widest, sync = topo.device_level_tables(layout.device)
-        status = _lib.lib().dqz_bp_sweep_levels(
-            layout.gptr, T.data_ptr(), n2e_old.data_ptr(), e2n_old.data_ptr(), n2e_new.data_ptr(), e2n_new.data_ptr(),
-            src_sel.data_ptr(), edge_new.data_ptr(), flat.data_ptr(), off.data_ptr(), len(topo.levels), widest,
-            max_slice, max_chi, sync.data_ptr(), error_flag(layout.device).data_ptr(), stream)
+        if max_chi >= SLICED_MIN_CHI:
+            # large bonds: every (half-edge, slice) of a level is a work item, so a
+            # level of a few half-edges still spreads over the whole GPU
+            ih, isl, ioff, widest_items = topo.device_slice_items(layout, layout.device)
+            status = _lib.lib().dqz_bp_sweep_sliced(
+                layout.gptr, T.data_ptr(), n2e_old.data_ptr(), e2n_old.data_ptr(), n2e_new.data_ptr(),
+                e2n_new.data_ptr(), src_sel.data_ptr(), edge_new.data_ptr(), flat.data_ptr(), off.data_ptr(),
+                ih.data_ptr(), isl.data_ptr(), ioff.data_ptr(), len(topo.levels), widest_items, max_slice, max_chi,
+                sync.data_ptr(), error_flag(layout.device).data_ptr(), stream)
+        else:
+            status = _lib.lib().dqz_bp_sweep_levels(
+                layout.gptr, T.data_ptr(), n2e_old.data_ptr(), e2n_old.data_ptr(), n2e_new.data_ptr(),
+                e2n_new.data_ptr(), src_sel.data_ptr(), edge_new.data_ptr(), flat.data_ptr(), off.data_ptr(),
+                len(topo.levels), widest, max_slice, max_chi, sync.data_ptr(), error_flag(layout.device).data_ptr(),
+                stream)
         if status == _lib.DQZ_OK:
             if mid_event is not None:
                 mid_event.record(torch.cuda.current_stream())

@@ -161,6 +161,19 @@ int dqz_bp_sweep_levels(const dqz_graph_t *g, const void *tensors, const void *n
                         int32_t max_slice, int32_t max_chi, uint32_t *sync, int32_t *error_flag,
                         cudaStream_t stream);
 
+/* The same sweep for large bonds: the work items of level l are
+ * (item_half[i], item_slice[i]) for i in item_off[l] .. item_off[l+1] (every
+ * slice of the bond of every half-edge of the level), spread over the grid;
+ * each writes one column of its unnormalised message, then a second barrier
+ * pass divides each message of the level by its trace. Bit-identical to the
+ * per-level launches; max_items bounds the items of one level. */
+int dqz_bp_sweep_sliced(const dqz_graph_t *g, const void *tensors, const void *n2e_old, const void *e2n_old,
+                        void *n2e_new, void *e2n_new, const uint8_t *src_sel, const uint8_t *edge_new,
+                        const int32_t *halves, const int32_t *level_off, const int32_t *item_half,
+                        const int32_t *item_slice, const int32_t *item_off, int32_t n_levels, int32_t max_items,
+                        int32_t max_slice, int32_t max_chi, uint32_t *sync, int32_t *error_flag,
+                        cudaStream_t stream);
+
 /* Edge pass on complex64 messages (see dqz_bp_edge_pass). */
 int dqz_bp_edge_pass_c64(const dqz_graph_t *g, const void *n2e_old, const void *n2e_new,
                          const uint8_t *edge_new, void *e2n_new, cudaStream_t stream);
@@ -308,8 +321,9 @@ int dqz_apply_half_gates(const void *tensors_in, void *tensors_out, const int64_
  * Writes Gamma tensors in place (capacity layout), lambdas, edge_chi, and
  * err/entropy per job. max_rows / max_cols bound the rows (d x the other
  * bonds) and columns (bond x gate rank) of the jobs' matrices.
- * Jobs with a 256-row matrix or more run, where their matrices fit in shared
- * memory, on an on-chip form (a cluster of two CTAs per job, one per side);
+ * In batches of at most one job per SM, jobs with a 256-row matrix or more run,
+ * where their matrices fit in shared memory, on an on-chip form (a cluster of
+ * two CTAs per job, one per side: lower latency);
  * the others on a one-CTA kernel with its matrices in `scratch`. The scratch
  * (dqz_simple_update_scratch_bytes) also holds one byte per job recording
  * which form did it. Knob DQZ_TUNE_SU_ONCHIP = 1 sends every job to the

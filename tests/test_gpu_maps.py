@@ -359,19 +359,22 @@ def test_gauge_knobs_leave_results_unchanged_and_tuner_caches(tmp_path):
         autotune.set_knobs({k: 0 for k in autotune.KNOBS})
 
 
-@pytest.mark.parametrize("case", ["lattice_3x3x3", "eagle_cell"])
+@pytest.mark.parametrize("case", ["lattice_3x3x3", "eagle_cell_4", "eagle_cell_8_16", "eagle_cell_32"])
 def test_one_launch_sweep_equals_level_launches(case):
-    """dqz_bp_sweep_levels (every node level of the asynchronous DFS schedule
-    and the edge pass in one cooperative launch, grid barriers between levels)
-    gives one dqz_bp_node_update launch per level plus dqz_bp_edge_pass, bit
-    for bit, over several sweeps."""
+    """The one-launch asynchronous sweep (every node level of the DFS schedule
+    and the edge pass in one cooperative launch, grid barriers between levels:
+    dqz_bp_sweep_levels below bond 8, dqz_bp_sweep_sliced with one work item
+    per bond slice from bond 8) gives one dqz_bp_node_update launch per level
+    plus dqz_bp_edge_pass, bit for bit, over several sweeps; mixed bonds of 8
+    and 16 give levels of uneven item counts."""
     from dequantizer_b200 import _lib
     from dequantizer_b200.layout import GraphLayout
 
     g = G.get_nd_lattice([3, 3, 3], 2, 2) if case == "lattice_3x3x3" else G.get_heavy_hex_ibm_eagle_lattice_infinite()
-    if case == "eagle_cell":
+    if case.startswith("eagle_cell"):
+        rng = np.random.default_rng(5)
         for e in g.edges.values():
-            e.dimension = 4
+            e.dimension = {"eagle_cell_4": 4, "eagle_cell_32": 32}.get(case) or int(rng.choice([8, 16]))
         g.refresh_bond_shapes()
     tensors = random_tensors(g, 21)
     msgs = random_messages(g, 22)
@@ -383,6 +386,17 @@ def test_one_launch_sweep_equals_level_launches(case):
     e2n = L.pack_messages([torch.from_numpy(msgs[MessageID(e.id, nd.id)]).cuda() for nd, e in topo.half_ids()])
     src_sel, edge_new, levels = topo.device_tables(T.device)
     stream = _lib.stream_handle()
+    if L.max_chi() >= M.SLICED_MIN_CHI:
+        # the sliced kernel itself accepts the schedule (no per-level fallback)
+        flat, off, _, sync = topo.device_level_tables(T.device)
+        ih, isl, ioff, widest = topo.device_slice_items(L, T.device)
+        na, ea = torch.zeros_like(n2e), torch.zeros_like(e2n)
+        status = _lib.lib().dqz_bp_sweep_sliced(
+            L.gptr, T.data_ptr(), n2e.data_ptr(), e2n.data_ptr(), na.data_ptr(), ea.data_ptr(), src_sel.data_ptr(),
+            edge_new.data_ptr(), flat.data_ptr(), off.data_ptr(), ih.data_ptr(), isl.data_ptr(), ioff.data_ptr(),
+            len(topo.levels), widest, L.max_slice(), L.max_chi(), sync.data_ptr(),
+            M.error_flag(T.device).data_ptr(), stream)
+        assert status == _lib.DQZ_OK
     a = (n2e.clone(), e2n.clone())
     b = (n2e.clone(), e2n.clone())
     for _ in range(3):
