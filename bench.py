@@ -550,6 +550,8 @@ def workload_suite(args):
                         "uniform_bond_16": bool(ba.layout.uniform_k3_chi() == 16),
                         "fp64_sweeps_per_regauge": float(np.mean(ba.bp_iterations[n0:])),
                         "bf16_sweeps_per_regauge": (float(np.mean(ba.bf16_sweeps[b0:])) if ba.bf16_sweeps[b0:]
+                                                    else 0.0),
+                        "fp32_sweeps_per_regauge": (float(np.mean(ba.fp32_sweeps[b0:])) if ba.fp32_sweeps[b0:]
                                                     else 0.0)}
         del ba
         torch.cuda.empty_cache()
@@ -742,7 +744,8 @@ def run_anneal(args, world, rank, local):
             "metric": METRIC, "workload": "batched annealing", "value": world * len(energies) * args.steps / elapsed,
             "unit": "instance-steps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": elapsed / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
-            "dtype": "c128" if args.anneal_precision == "fp64" else "bf16 regauge sweeps + c128", "data": "synthetic",
+            "dtype": "c128" if args.anneal_precision == "fp64" else "bf16 + fp32 regauge sweeps + c128",
+            "data": "synthetic",
             "config": {"instances": args.instances, "nodes": int(sum(sizes)), "chi": args.chi,
                        "trotter_steps": n_steps, "dt": dt, "order": 2, "bp_accuracy": 1e-5,
                        "bp_schedule": "synchronous, per-instance convergence"},
@@ -752,6 +755,8 @@ def run_anneal(args, world, rank, local):
                                             "max": int(np.max(ba.bp_iterations[sw0:]))},
             "precision": args.anneal_precision,
             "bf16_sweeps_per_regauge_rank0": (float(np.mean(ba.bf16_sweeps[bf0:])) if ba.bf16_sweeps[bf0:]
+                                              else None),
+            "fp32_sweeps_per_regauge_rank0": (float(np.mean(ba.fp32_sweeps[bf0:])) if ba.fp32_sweeps[bf0:]
                                               else None),
             "clocks": clk.summary(),
         }), flush=True)

@@ -54,6 +54,8 @@ class BatchedAnnealer:
         precision: str = "fp64",
         bf16_handover: float = 2e-4,
         bf16_max_sweeps: int = 40,
+        fp32_handover: float = 1e-7,
+        fp32_max_sweeps: int = 60,
     ):
         """``autotune``: time the gauge kernels' launch shapes on the first
         regauge of every new maximal bond dimension (``autotune.tune_gauge``,
@@ -64,10 +66,15 @@ class BatchedAnnealer:
         accumulation, complex64 messages) on the instances above the accuracy,
         with no gauge or distance evaluation, until an instance's mean change of
         its node->edge messages per sweep falls to ``bf16_handover`` (at most
-        ``bf16_max_sweeps``); the FP64 loop of the reference (sweep, Vidal gauge,
-        Vidal distance until the accuracy) then finishes from there. Eigen and
-        singular value decompositions, the distances and the gates stay FP64.
-        ``precision="fp64"`` is the plain form."""
+        ``bf16_max_sweeps``), then FP32 sweeps (dqz_bp_node_update_k3,
+        complex64) until it falls to ``fp32_handover`` (at most
+        ``fp32_max_sweeps``; BF16 products settle near 5e-5, FP32 ones near
+        1e-7); the FP64 loop of the reference (sweep, Vidal gauge, Vidal
+        distance until the accuracy) then finishes from there, normally after
+        one pass, since the gauge and distance evaluations of the sweeps in
+        between are skipped. Eigen and singular value decompositions, the
+        distances and the gates stay FP64. ``precision="fp64"`` is the plain
+        form."""
         if schedule not in ("sync", "flooding"):
             raise ValueError("batched annealing runs the synchronous or flooding BP schedule")
         if precision not in ("fp64", "mixed"):
@@ -75,7 +82,10 @@ class BatchedAnnealer:
         self.precision = precision
         self.bf16_handover = float(bf16_handover)
         self.bf16_max_sweeps = int(bf16_max_sweeps)
+        self.fp32_handover = float(fp32_handover)
+        self.fp32_max_sweeps = int(fp32_max_sweeps)
         self.bf16_sweeps: List[List[int]] = []
+        self.fp32_sweeps: List[List[int]] = []
         if not torch.cuda.is_available():
             raise RuntimeError("BatchedAnnealer runs on the GPU only")
         _lib.lib()
@@ -262,9 +272,11 @@ class BatchedAnnealer:
         return G, lam
 
     def _bf16_prephase(self, T, n2e, e2n, active: np.ndarray):
-        """BF16 tensor-core sweeps of the listed instances (complex64 messages)
-        until each one's mean node->edge message change per sweep is at most
-        ``bf16_handover``; returns complex128 message arenas for the FP64 loop.
+        """Low-precision sweeps of the listed instances (complex64 messages),
+        no gauge or distance evaluation: BF16 tensor-core sweeps until each
+        one's mean node->edge message change per sweep is at most
+        ``bf16_handover``, then FP32 sweeps until it is at most
+        ``fp32_handover``; returns complex128 message arenas for the FP64 loop.
         Instances not listed keep their messages."""
         L = self.layout
         dev = L.device
@@ -280,25 +292,40 @@ class BatchedAnnealer:
         a, b = n2e.to(torch.complex64), e2n.to(torch.complex64)
         flag = error_flag(dev)
         change = torch.empty(max(L.n_halves, 1), dtype=torch.float64, device=dev)
-        sweeps = np.zeros(self.n_inst, dtype=np.int64)
-        active = active.copy()
-        for _ in range(self.bf16_max_sweeps):
+
+        def stage(active, handover, max_sweeps, update):
+            nonlocal a, b
+            sweeps = np.zeros(self.n_inst, dtype=np.int64)
+            for _ in range(max_sweeps):
+                if not active.any():
+                    break
+                a_new, b_new = a.clone(), torch.empty_like(b)
+                update(active, a, b, a_new)
+                _lib.call("dqz_bp_edge_pass_c64", L.gptr, a.data_ptr(), a_new.data_ptr(), edge_new.data_ptr(),
+                          b_new.data_ptr(), stream)
+                _lib.call("dqz_message_changes_c64", L.gptr, a_new.data_ptr(), a.data_ptr(), change.data_ptr(),
+                          stream)
+                sums = torch.zeros(self.n_inst, dtype=torch.float64, device=dev)
+                sums.index_add_(0, self.inst_id_half, change[: L.n_halves])
+                mean_change = (sums / self._halves_per_inst).cpu().numpy()
+                a, b = a_new, b_new
+                sweeps += active
+                active = active & (mean_change > handover)
+            return sweeps
+
+        def bf16_update(active, a, b, a_new):
             nodes = torch.from_numpy(self._ranges(self.node_bounds, active)).to(dev)
-            a_new, b_new = a.clone(), torch.empty_like(b)
             _lib.call("dqz_bp_node_update_k3_umma", L.gptr, self._T_bf16.data_ptr(), a.data_ptr(), b.data_ptr(),
                       a_new.data_ptr(), src_sel.data_ptr(), nodes.data_ptr(), nodes.numel(), flag.data_ptr(), stream)
-            _lib.call("dqz_bp_edge_pass_c64", L.gptr, a.data_ptr(), a_new.data_ptr(), edge_new.data_ptr(),
-                      b_new.data_ptr(), stream)
-            _lib.call("dqz_message_changes_c64", L.gptr, a_new.data_ptr(), a.data_ptr(), change.data_ptr(), stream)
-            sums = torch.zeros(self.n_inst, dtype=torch.float64, device=dev)
-            sums.index_add_(0, self.inst_id_half, change[: L.n_halves])
-            mean_change = (sums / self._halves_per_inst).cpu().numpy()
-            a, b = a_new, b_new
-            sweeps += active
-            active &= mean_change > self.bf16_handover
-            if not active.any():
-                break
-        self.bf16_sweeps.append(sweeps.tolist())
+
+        def fp32_update(active, a, b, a_new):
+            halves = torch.from_numpy(self._ranges(self.half_bounds, active)).to(dev)
+            _lib.call("dqz_bp_node_update_k3", L.gptr, 16, 32, T32.data_ptr(), a.data_ptr(), b.data_ptr(),
+                      a_new.data_ptr(), src_sel.data_ptr(), halves.data_ptr(), halves.numel(), flag.data_ptr(),
+                      stream)
+
+        self.bf16_sweeps.append(stage(active.copy(), self.bf16_handover, self.bf16_max_sweeps, bf16_update).tolist())
+        self.fp32_sweeps.append(stage(active.copy(), self.fp32_handover, self.fp32_max_sweeps, fp32_update).tolist())
         return a.to(torch.complex128), b.to(torch.complex128)
 
     def _sweep_halves(self, T, n2e, e2n, n2e_new, e2n_new, halves):

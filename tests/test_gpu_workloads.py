@@ -189,9 +189,10 @@ def test_batched_measurement_sampling_equals_independent_runs():
 
 def test_mixed_precision_batched_annealer_tracks_fp64():
     """BatchedAnnealer(precision="mixed"): once every bond has dimension 16,
-    each regauge starts with BF16 tensor-core sweeps and hands over to the
-    FP64 loop of the reference; the densities stay within 1e-4 of the FP64
-    annealer's (the FP64 loop finishes every regauge to the same accuracy)."""
+    each regauge starts with BF16 tensor-core sweeps, then FP32 sweeps, and
+    hands over to the FP64 loop of the reference; the densities stay within
+    1e-4 of the FP64 annealer's (the FP64 loop finishes every regauge to the
+    same accuracy)."""
     from dequantizer_b200.annealing import BatchedAnnealer
 
     energies = [W.random_regular_energy(n, 3, seed=60 + n, field_std=0.5) for n in (16, 20, 24)]
@@ -204,6 +205,7 @@ def test_mixed_precision_batched_annealer_tracks_fp64():
     mixed = runs["mixed"][1]
     assert mixed.layout.uniform_k3_chi() == 16
     assert sum(sum(s) for s in mixed.bf16_sweeps) > 0, "no regauge took the BF16 path"
+    assert sum(sum(s) for s in mixed.fp32_sweeps) > 0, "no regauge took the FP32 stage"
     for k in range(len(energies)):
         assert np.abs(runs["mixed"][0][k] - runs["fp64"][0][k]).max() < 1e-4
     assert int(M.error_flag(torch.device("cuda", 0)).item()) == 0
