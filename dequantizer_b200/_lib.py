@@ -109,6 +109,8 @@ _SIGNATURES = {
     "dqz_vidal_edges": (ctypes.c_int, [_G, _P, _D, _P, _P, _I, _P, _I, _P, _P]),
     "dqz_vidal_edges_scratch_bytes": (_S, [_I, _I]),
     "dqz_absorb": (ctypes.c_int, [_G, _P, _P, _P, _I, _P, _I, _P, _P]),
+    "dqz_absorb_split": (ctypes.c_int, [_G, _P, _P, _P, ctypes.c_int64, _P, _I, _P, _P]),
+    "dqz_absorb_split_scratch_bytes": (_S, [_I]),
     "dqz_absorb_scratch_bytes": (_S, [_I, _I]),
     "dqz_absorb_k3": (ctypes.c_int, [_G, _I, _P, _P, _P, _P, _I, _P, _P]),
     "dqz_vidal_distance": (ctypes.c_int, [_G, _P, _P, _D, _P, _P, _I, _I, _P, _I, _P]),

@@ -299,8 +299,117 @@ __global__ void __launch_bounds__(GAUGE_THREADS) absorb_kernel(dqz_graph_t g, co
   }
 }
 
+// Nodes too large for shared memory: one CTA per (node, j), j the output
+// index of the node's first bond. X = sum_a orth_0[a][j] T[a, ..] (the first
+// mode product restricted to j, T read through L2), then the other bonds'
+// mode products on X in shared memory, each element computed as the
+// whole-tensor mode products compute it; X is written unnormalised and its
+// squared norm to partial[it * DQZ_MAX_CHI + j]. absorb_scale_kernel then
+// divides each node by the square root of its partials' sum (j order).
+__global__ void __launch_bounds__(GAUGE_THREADS) absorb_split_kernel(dqz_graph_t g, const cd *__restrict__ Tin,
+                                                                      const cd *__restrict__ orth,
+                                                                      cd *__restrict__ Tout, long long max_slice,
+                                                                      double *partial,
+                                                                      const int32_t *__restrict__ sel) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double *red = reinterpret_cast<double *>(smem_raw);
+  cd *bufA = reinterpret_cast<cd *>(smem_raw + 48 * sizeof(double));
+  cd *bufB = bufA + max_slice;
+  const int it = blockIdx.x, j = blockIdx.y;
+  const int v = sel ? sel[it] : it;
+  NodeShape s;
+  load_shape(g, v, s);
+  const int c0 = s.k > 0 ? s.dims[0] : 1;
+  if (j >= c0) return;
+  const long long P0 = s.size / c0;
+  const cd *T = Tin + g.node_off[v];
+  if (s.k > 0) {
+    const cd *G0 = orth + g.half_msg_off[s.half0];
+    for (long long r = threadIdx.x; r < P0; r += blockDim.x) {
+      cd acc = czero();
+      for (int b = 0; b < c0; ++b) cfma(acc, G0[b * c0 + j], T[b * P0 + r]);
+      bufA[r] = acc;
+    }
+  } else {
+    for (long long r = threadIdx.x; r < P0; r += blockDim.x) bufA[r] = T[r];
+  }
+  __syncthreads();
+  cd *cur = bufA, *nxt = bufB;
+  long long L = 1;
+  for (int f = 1; f < s.k; ++f) {
+    const int q = s.dims[f];
+    const long long R = P0 / L / q;
+    mode_product<false>(cur, nxt, L, q, q, R, orth + g.half_msg_off[s.half0 + f], 1, q);
+    __syncthreads();
+    cd *t = cur;
+    cur = nxt;
+    nxt = t;
+    L *= q;
+  }
+  double n2 = 0.0;
+  cd *O = Tout + g.node_off[v] + (long long)j * P0;
+  for (long long r = threadIdx.x; r < P0; r += blockDim.x) {
+    n2 += cabs2(cur[r]);
+    O[r] = cur[r];
+  }
+  n2 = block_sum(n2, red);
+  if (threadIdx.x == 0) partial[(long long)it * DQZ_MAX_CHI + j] = n2;
+}
+
+__global__ void __launch_bounds__(GAUGE_THREADS) absorb_scale_kernel(dqz_graph_t g, cd *Tout,
+                                                                      const double *__restrict__ partial,
+                                                                      const int32_t *__restrict__ sel) {
+  __shared__ double inv_sh;
+  const int it = blockIdx.x;
+  const int v = sel ? sel[it] : it;
+  NodeShape s;
+  load_shape(g, v, s);
+  if (threadIdx.x == 0) {
+    const int c0 = s.k > 0 ? s.dims[0] : 1;
+    double n2 = 0.0;
+    for (int j = 0; j < c0; ++j) n2 += partial[(long long)it * DQZ_MAX_CHI + j];
+    inv_sh = 1.0 / sqrt(n2);
+  }
+  __syncthreads();
+  const double inv = inv_sh;
+  cd *O = Tout + g.node_off[v];
+  for (long long i = threadIdx.x; i < s.size; i += blockDim.x) O[i] = cscale(O[i], inv);
+}
+
 // ---------------------------------------------------------- vidal distance
-// partial[h] = trace norm of (R/tr R - ideal) for bond e of node v (h = (v,e)).
+// partial[h] = trace norm of (R/tr R - ideal) for bond e of node v (h = (v,e)),
+// one CTA per half-edge. R = Y^H Y with Y[x][a] = T[.., a@e, ..](x) *
+// prod_{f != e} lambda_f[idx_f(x)] (the lambda^2-weighted reduced matrix). The
+// bond slice is staged through shared memory VDT_CHUNK elements at a time
+// (rows x padded columns, row stride cp + 1: conflict-free column reads); R
+// is register-tiled: each thread accumulates a 4 x 4 tile of the upper
+// triangle of R (tiles ti <= tj) over every `splits`-th row of the chunk, 16
+// complex FMAs per 8 shared loads, and the splits' tiles are summed in index
+// order at the end. The trace norm comes from the eigenvalues of the
+// Hermitian matrix (herm_eigh without vectors).
+constexpr int VDT_CHUNK = 2048;            // staged elements per chunk
+constexpr int VDT_PART = GAUGE_THREADS * 16;  // split partial tiles (cd)
+
+__host__ __device__ inline int vdt_cp(int c) { return (c + 3) & ~3; }
+__host__ __device__ inline int vdt_rows(int c) {
+  const int r = VDT_CHUNK / vdt_cp(c);
+  return r < 1 ? 1 : r;
+}
+__host__ __device__ inline size_t vdt_union_elems(int c) {
+  const size_t y = (size_t)vdt_rows(c) * (vdt_cp(c) + 1);
+  return y > (size_t)VDT_PART ? y : (size_t)VDT_PART;
+}
+// eigh header | union(Y chunk, split partials) | row weights | R | w
+__host__ __device__ inline size_t vdt_smem(int max_chi) {
+  int rmax = 0;
+  for (int c = 1; c <= max_chi; ++c) rmax = vdt_rows(c) > rmax ? vdt_rows(c) : rmax;
+  size_t u = 0;
+  for (int c = 1; c <= max_chi; ++c) u = vdt_union_elems(c) > u ? vdt_union_elems(c) : u;
+  return round16(48 * sizeof(double) + (DQZ_MAX_CHI / 2 + 1) * sizeof(Rot)) + u * sizeof(cd) +
+         round16((size_t)rmax * sizeof(double)) + (size_t)max_chi * max_chi * sizeof(cd) +
+         (size_t)max_chi * sizeof(double);
+}
+
 __global__ void __launch_bounds__(GAUGE_THREADS) vidal_distance_kernel(dqz_graph_t g, const cd *__restrict__ Tall,
                                                                         const double *__restrict__ lambdas,
                                                                         double eps, double *partial, int max_chi,
@@ -308,13 +417,20 @@ __global__ void __launch_bounds__(GAUGE_THREADS) vidal_distance_kernel(dqz_graph
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double *red = reinterpret_cast<double *>(smem_raw);
   Rot *rots = reinterpret_cast<Rot *>(smem_raw + 48 * sizeof(double));
-  cd *Rm = reinterpret_cast<cd *>(rots + (DQZ_MAX_CHI / 2 + 1));
-  cd *Vm = Rm + max_chi * max_chi;
-  double *w = reinterpret_cast<double *>(Vm + max_chi * max_chi);
+  cd *U = reinterpret_cast<cd *>(smem_raw + round16(48 * sizeof(double) + (DQZ_MAX_CHI / 2 + 1) * sizeof(Rot)));
+  size_t umax = 0;
+  int rmax = 0;
+  for (int c = 1; c <= max_chi; ++c) {
+    umax = vdt_union_elems(c) > umax ? vdt_union_elems(c) : umax;
+    rmax = vdt_rows(c) > rmax ? vdt_rows(c) : rmax;
+  }
+  double *wrow = reinterpret_cast<double *>(U + umax);
+  cd *Rm = reinterpret_cast<cd *>(reinterpret_cast<unsigned char *>(wrow) + round16((size_t)rmax * sizeof(double)));
+  double *w = reinterpret_cast<double *>(Rm + max_chi * max_chi);
   __shared__ cd trace_sh;
   __shared__ int count_sh;
   const int total = sel ? n_sel : g.n_halves;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int tid = threadIdx.x;
   for (int it = blockIdx.x; it < total; it += gridDim.x) {
     const int h = sel ? sel[it] : it;
     const int v = g.half_node[h];
@@ -327,59 +443,112 @@ __global__ void __launch_bounds__(GAUGE_THREADS) vidal_distance_kernel(dqz_graph
     const long long P = s.size / ce;
     const double *lam[DQZ_MAX_DEGREE];
     for (int f = 0; f < s.k; ++f) lam[f] = lambdas + g.edge_lam_off[g.half_edge[s.half0 + f]];
-    const int npair = ce * (ce + 1) / 2;
-    for (int pi = warp; pi < npair; pi += nw) {
-      // pair index -> (ap <= a)
-      int ap = 0, rem = pi;
-      while (rem >= ce - ap) {
-        rem -= ce - ap;
-        ++ap;
-      }
-      const int a = ap + rem;
-      cd acc = czero();
-      for (long long x = lane; x < P; x += 32) {
+    const int cp = vdt_cp(ce), ld = cp + 1, rows = vdt_rows(ce);
+    const int nt = cp / 4, ntl = nt * (nt + 1) / 2;
+    const int splits = GAUGE_THREADS / ntl;  // >= 1: ntl <= 136
+    const int tile = tid % ntl, split = tid / ntl;
+    const bool active = split < splits;
+    int ti = 0, rem = tile;
+    while (rem >= nt - ti) {
+      rem -= nt - ti;
+      ++ti;
+    }
+    const int tj = ti + rem;
+    cd acc[4][4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+#pragma unroll
+      for (int m = 0; m < 4; ++m) acc[k][m] = czero();
+    for (long long x0 = 0; x0 < P; x0 += rows) {
+      const int nr = (int)((P - x0) < rows ? (P - x0) : rows);
+      for (int xl = tid; xl < nr; xl += GAUGE_THREADS) {
+        const long long x = x0 + xl;
         const long long l = x / Re, r = x - l * Re;
-        const long long o0 = (l * ce) * Re + r;  // offset with a_e = 0
+        const long long o0 = (l * ce) * Re + r;
         double wt = 1.0;
         for (int f = 0; f < s.k; ++f) {
           if (f == e) continue;
-          const int idx = (int)((o0 / s.stride[f]) % s.dims[f]);
-          const double lv = lam[f][idx];
-          wt *= lv * lv;
+          wt *= lam[f][(int)((o0 / s.stride[f]) % s.dims[f])];
         }
-        cfmac(acc, T[o0 + ap * Re], cscale(T[o0 + a * Re], wt));
+        wrow[xl] = wt;
       }
-      acc = warp_csum(acc);
-      if (lane == 0) {
-        Rm[ap * ce + a] = acc;
-        Rm[a * ce + ap] = cconj(acc);
+      __syncthreads();
+      for (int q = tid; q < nr * cp; q += GAUGE_THREADS) {
+        const int xl = q % nr, a = q / nr;
+        cd y = czero();
+        if (a < ce) {
+          const long long x = x0 + xl;
+          const long long l = x / Re, r = x - l * Re;
+          y = cscale(T[(l * ce + a) * Re + r], wrow[xl]);
+        }
+        U[xl * ld + a] = y;
+      }
+      __syncthreads();
+      if (active) {
+        for (int xl = split; xl < nr; xl += splits) {
+          const cd *row = U + xl * ld;
+          cd yi[4], yj[4];
+#pragma unroll
+          for (int k = 0; k < 4; ++k) {
+            yi[k] = row[4 * ti + k];
+            yj[k] = row[4 * tj + k];
+          }
+#pragma unroll
+          for (int k = 0; k < 4; ++k)
+#pragma unroll
+            for (int m = 0; m < 4; ++m) cfmac(acc[k][m], yi[k], yj[m]);
+        }
+      }
+      __syncthreads();
+    }
+    // the splits' tiles, summed in split order
+    if (active) {
+#pragma unroll
+      for (int k = 0; k < 4; ++k)
+#pragma unroll
+        for (int m = 0; m < 4; ++m) U[(split * ntl + tile) * 16 + k * 4 + m] = acc[k][m];
+    }
+    __syncthreads();
+    for (int q = tid; q < ntl * 16; q += GAUGE_THREADS) {
+      const int tl = q / 16, km = q % 16;
+      cd sum = U[tl * 16 + km];
+      for (int sp = 1; sp < splits; ++sp) sum = cadd(sum, U[(sp * ntl + tl) * 16 + km]);
+      int a = 0, rr = tl;
+      while (rr >= nt - a) {
+        rr -= nt - a;
+        ++a;
+      }
+      const int i = 4 * a + km / 4, j = 4 * (a + rr) + km % 4;
+      if (i < ce && j < ce && i <= j) {
+        Rm[i * ce + j] = sum;
+        if (i < j) Rm[j * ce + i] = cconj(sum);
       }
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
+    if (tid == 0) {
       cd tr = czero();
       for (int i = 0; i < ce; ++i) tr = cadd(tr, Rm[i * ce + i]);
       trace_sh = tr;
     }
     __syncthreads();
     const cd tr = trace_sh;
-    for (int i = threadIdx.x; i < ce * ce; i += blockDim.x) Rm[i] = cdiv(Rm[i], tr);
+    for (int i = tid; i < ce * ce; i += blockDim.x) Rm[i] = cdiv(Rm[i], tr);
     __syncthreads();
-    if (threadIdx.x == 0) {
+    if (tid == 0) {
       int cnt = 0;
       for (int i = 0; i < ce; ++i) cnt += Rm[i * ce + i].x > eps ? 1 : 0;
       count_sh = cnt;
     }
     __syncthreads();
     const double idv = 1.0 / (double)count_sh;
-    for (int i = threadIdx.x; i < ce; i += blockDim.x)
+    for (int i = tid; i < ce; i += blockDim.x)
       if (Rm[i * ce + i].x > eps) Rm[i * ce + i].x -= idv;
     __syncthreads();
-    herm_eigh(Rm, ce, Vm, ce, ce, w, rots, red);
+    herm_eigh(Rm, ce, nullptr, ce, ce, w, rots, red);
     double t = 0.0;
-    for (int i = threadIdx.x; i < ce; i += blockDim.x) t += fabs(w[i]);
+    for (int i = tid; i < ce; i += blockDim.x) t += fabs(w[i]);
     t = block_sum(t, red);
-    if (threadIdx.x == 0) partial[h] = t;
+    if (tid == 0) partial[h] = t;
     __syncthreads();
   }
 }
@@ -673,6 +842,30 @@ extern "C" int dqz_absorb(const dqz_graph_t *g, const void *tensors_in, const vo
   return DQZ_OK;
 }
 
+extern "C" size_t dqz_absorb_split_scratch_bytes(int32_t n_nodes) {
+  return (size_t)(n_nodes > 0 ? n_nodes : 0) * DQZ_MAX_CHI * sizeof(double);
+}
+
+extern "C" int dqz_absorb_split(const dqz_graph_t *g, const void *tensors_in, const void *orth, void *tensors_out,
+                                int64_t max_slice, const int32_t *nodes, int32_t n_sel, void *scratch,
+                                cudaStream_t stream) {
+  if (!g || !tensors_in || !orth || !tensors_out || !scratch || max_slice <= 0) return DQZ_ERR_ARG;
+  if (tensors_in == tensors_out) return DQZ_ERR_ARG;
+  if (nodes && (n_sel < 0 || n_sel > g->n_nodes)) return DQZ_ERR_ARG;
+  const int total = nodes ? n_sel : g->n_nodes;
+  if (total == 0) return DQZ_OK;
+  if (max_slice < DQZ_MAX_PHYS) max_slice = DQZ_MAX_PHYS;  // a node without bonds is its own slice
+  const size_t smem = 48 * sizeof(double) + 2 * (size_t)max_slice * sizeof(cd);
+  if (smem > SMEM_LIMIT) return DQZ_ERR_UNSUPPORTED;
+  DQZ_SMEM_ATTR_ONCE(absorb_split_kernel, SMEM_LIMIT);
+  absorb_split_kernel<<<dim3(total, DQZ_MAX_CHI), GAUGE_THREADS, smem, stream>>>(
+      *g, (const cd *)tensors_in, (const cd *)orth, (cd *)tensors_out, (long long)max_slice, (double *)scratch, nodes);
+  DQZ_CHECK_LAUNCH();
+  absorb_scale_kernel<<<total, GAUGE_THREADS, 0, stream>>>(*g, (cd *)tensors_out, (const double *)scratch, nodes);
+  DQZ_CHECK_LAUNCH();
+  return DQZ_OK;
+}
+
 extern "C" int dqz_vidal_distance(const dqz_graph_t *g, const void *tensors, const double *lambdas, double eps,
                                   double *partial, double *out, int32_t max_chi, int32_t max_slice,
                                   const int32_t *halves, int32_t n_sel, cudaStream_t stream) {
@@ -693,7 +886,7 @@ extern "C" int dqz_vidal_distance(const dqz_graph_t *g, const void *tensors, con
       vidal_distance_warp_kernel<<<(total + wpb - 1) / wpb, 32 * wpb, wpb * per, stream>>>(
           *g, (const cd *)tensors, lambdas, eps, partial, max_chi, halves, total);
     } else {
-      size_t smem = eigh_smem(max_chi) + 2 * (size_t)max_chi * max_chi * sizeof(cd) + (size_t)max_chi * sizeof(double);
+      const size_t smem = vdt_smem(max_chi);
       DQZ_SMEM_ATTR_ONCE(vidal_distance_kernel, SMEM_LIMIT);
       vidal_distance_kernel<<<total, GAUGE_THREADS, smem, stream>>>(*g, (const cd *)tensors, lambdas, eps, partial,
                                                                     max_chi, halves, total);

@@ -67,8 +67,8 @@ __device__ __forceinline__ bool jacobi_rot(double a, double b, cd c, Rot &r) {
 
 // Hermitian eigendecomposition. A (n x n, row-major, lda) is destroyed; on
 // return w[i] holds eigenvalue i and column i of V (row-major, ldv) the
-// matching eigenvector (unsorted). rots: >= n/2+1 entries, red: 33 doubles,
-// all in shared memory.
+// matching eigenvector (unsorted); V may be null (eigenvalues only, the same
+// values). rots: >= n/2+1 entries, red: 33 doubles, all in shared memory.
 // The input is first made exactly Hermitian ((A + A^H) / 2, real diagonal):
 // an anti-Hermitian rounding residual is invisible to the rotations, which
 // read the upper triangle only, and would otherwise keep the off-diagonal
@@ -78,7 +78,8 @@ static __device__ void herm_eigh(cd *A, int lda, cd *V, int ldv, int n, double *
                           int max_sweeps = 40) {
   const int tid = threadIdx.x, nt = blockDim.x;
   __shared__ int rotated_sh;
-  for (int i = tid; i < n * n; i += nt) V[(i / n) * ldv + (i % n)] = (i / n == i % n) ? mk(1.0, 0.0) : czero();
+  if (V)
+    for (int i = tid; i < n * n; i += nt) V[(i / n) * ldv + (i % n)] = (i / n == i % n) ? mk(1.0, 0.0) : czero();
   for (int i = tid; i < n * n; i += nt) {
     const int r = i / n, c = i % n;
     if (r < c) {
@@ -136,10 +137,12 @@ static __device__ void herm_eigh(cd *A, int lda, cd *V, int ldv, int n, double *
           cd x = A[row * lda + r.p], y = A[row * lda + r.q];
           A[row * lda + r.p] = cadd(cmul(x, r.j00), cmul(y, r.j10));
           A[row * lda + r.q] = cadd(cmul(x, r.j01), cmul(y, r.j11));
-          x = V[row * ldv + r.p];
-          y = V[row * ldv + r.q];
-          V[row * ldv + r.p] = cadd(cmul(x, r.j00), cmul(y, r.j10));
-          V[row * ldv + r.q] = cadd(cmul(x, r.j01), cmul(y, r.j11));
+          if (V) {
+            x = V[row * ldv + r.p];
+            y = V[row * ldv + r.q];
+            V[row * ldv + r.p] = cadd(cmul(x, r.j00), cmul(y, r.j10));
+            V[row * ldv + r.q] = cadd(cmul(x, r.j01), cmul(y, r.j11));
+          }
         }
         __syncthreads();
         // A <- J^H A on rows (p, q)

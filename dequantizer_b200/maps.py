@@ -382,6 +382,16 @@ def vidal_gauge_packed(layout: GraphLayout, T, n2e, eps: float, out=None, edges=
         return G, lam
     ms = layout.max_size()
     nb = _lib.lib().dqz_absorb_scratch_bytes(nn, ms)
+    if nb and G.data_ptr() != T.data_ptr():
+        # nodes too large for shared memory: one CTA per (node, first-bond index)
+        part = _scratch(_lib.lib().dqz_absorb_split_scratch_bytes(nn), layout.device)
+        status = _lib.lib().dqz_absorb_split(layout.gptr, T.data_ptr(), orth.data_ptr(), G.data_ptr(),
+                                             layout.max_slice(), _lib.ptr(nodes), nn if nodes is not None else 0,
+                                             part.data_ptr(), stream)
+        if status == _lib.DQZ_OK:
+            return G, lam
+        if status != _lib.DQZ_ERR_UNSUPPORTED:
+            _lib.check("dqz_absorb_split", status)
     scratch = _scratch(nb, layout.device) if nb else None
     _lib.call("dqz_absorb", layout.gptr, T.data_ptr(), orth.data_ptr(), G.data_ptr(), ms, _lib.ptr(nodes),
               nn if nodes is not None else 0, _lib.ptr(scratch), stream)

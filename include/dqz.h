@@ -271,6 +271,16 @@ size_t dqz_vidal_edges_scratch_bytes(int32_t n_edges, int32_t max_chi);
 int dqz_absorb(const dqz_graph_t *g, const void *tensors_in, const void *orth, void *tensors_out,
                int32_t max_size, const int32_t *nodes, int32_t n_sel, void *scratch, cudaStream_t stream);
 size_t dqz_absorb_scratch_bytes(int32_t n_nodes, int32_t max_size);
+/* The same for nodes too large for shared memory, spread over one CTA per
+ * (node, output index of the node's first bond); every element is computed
+ * as dqz_absorb computes it, only the normalisation's sum runs in another
+ * order. max_slice bounds node size / first bond dimension (e.g. the largest
+ * bond slice); tensors_out must not be tensors_in; scratch holds
+ * dqz_absorb_split_scratch_bytes(n) bytes. DQZ_ERR_UNSUPPORTED when two
+ * slices do not fit in shared memory. Two launches. */
+int dqz_absorb_split(const dqz_graph_t *g, const void *tensors_in, const void *orth, void *tensors_out,
+                     int64_t max_slice, const int32_t *nodes, int32_t n_sel, void *scratch, cudaStream_t stream);
+size_t dqz_absorb_split_scratch_bytes(int32_t n_nodes);
 /* The same for degree-3 nodes with physical dimension 2 and every bond of
  * dimension chi (8 or 16), one CTA per node with the tensor held in shared
  * memory; needs no scratch. A node of any other shape is skipped and sets

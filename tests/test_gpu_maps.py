@@ -134,14 +134,25 @@ def test_symmetric_gauge_density_and_lambdas(case):
             assert rel_err(b, a) < TOL
 
 
-@pytest.mark.parametrize("case", ["small_bonds", "wide_slice", "large_bonds"])
+def _heavy_hex_mixed_bonds():
+    g = G.get_heavy_hex_ibm_eagle_lattice_infinite()
+    rng = np.random.default_rng(12)
+    for e in g.edges.values():
+        e.dimension = int(rng.choice([3, 17, 32]))
+    g.refresh_bond_shapes()
+    return g
+
+
+@pytest.mark.parametrize("case", ["small_bonds", "wide_slice", "large_bonds", "mixed_bonds"])
 def test_vidal_distance_matches_oracle(case):
     """small bonds and a wide bond slice (degree 4, chi 12: 3456-row slices
-    streamed in chunks): one warp per half-edge; bonds above 16 (chi 20): one
-    CTA per half-edge."""
+    streamed in chunks): one warp per half-edge; bonds above 16 (chi 20), and
+    the heavy-hex cell with bonds of 3, 17 and 32 (padded tiles, several
+    staged chunks): one CTA per half-edge."""
     g = {"small_bonds": lambda: G.get_nd_lattice([3, 2, 2], 2, 3),
          "wide_slice": lambda: G.get_nd_lattice([3, 3], 2, 12),
-         "large_bonds": lambda: G.get_random_regular_graph(6, 3, 2, 20, 3)}[case]()
+         "large_bonds": lambda: G.get_random_regular_graph(6, 3, 2, 20, 3),
+         "mixed_bonds": _heavy_hex_mixed_bonds}[case]()
     tensors = random_tensors(g, 9)
     rng = np.random.default_rng(10)
     lambdas = {eid: rng.uniform(0.1, 1, e.dimension) for eid, e in g.edges.items()}
@@ -216,6 +227,59 @@ def test_gauge_selection_updates_only_listed_entries():
     p, q = part.cpu().numpy(), part_full.cpu().numpy()
     assert np.array_equal(p[mask], q[mask])
     assert np.all(p[~mask] == -1.0)
+
+
+@pytest.mark.parametrize("mixed", [False, True])
+def test_split_absorb_matches_whole_node_absorb(mixed):
+    """dqz_absorb_split (nodes above shared memory: one CTA per node and
+    first-bond index) against dqz_absorb's global-scratch form on the heavy-hex
+    cell at bond 32 (or bonds of 3, 17 and 32) with arbitrary bond matrices:
+    the same elements up to the normalisation's summation order; with a node
+    list only the listed nodes are written."""
+    from dequantizer_b200 import _lib
+    from dequantizer_b200.layout import GraphLayout
+
+    g = _heavy_hex_mixed_bonds() if mixed else G.get_heavy_hex_ibm_eagle_lattice_infinite()
+    if not mixed:
+        for e in g.edges.values():
+            e.dimension = 32
+        g.refresh_bond_shapes()
+    tensors = random_tensors(g, 13)
+    topo = M.Topology(list(g.get_traversal_iterator()), True)
+    L = GraphLayout(topo.nodes, topo.edges, [e.dimension for e in topo.edges])
+    T = L.pack_tensors([torch.from_numpy(tensors[n.id]).cuda() for n in topo.nodes])
+    rng = np.random.default_rng(14)
+    orth = torch.zeros(max(L.msg_elems, 1), dtype=torch.complex128)
+    for h in range(L.n_halves):
+        c = int(L.edge_chi[L.half_edge[h]])
+        o = int(L.half_msg_off[h])
+        orth[o:o + c * c] = torch.from_numpy((rng.standard_normal((c, c)) + 1j * rng.standard_normal((c, c))).ravel())
+    orth = orth.cuda()
+    stream = _lib.stream_handle()
+    ms = L.max_size()
+    nb = _lib.lib().dqz_absorb_scratch_bytes(L.n_nodes, ms)
+    assert nb > 0, "the bond-32 nodes must exceed shared memory"
+    ref = torch.empty_like(T)
+    scratch = torch.empty(nb, dtype=torch.uint8, device=T.device)
+    _lib.call("dqz_absorb", L.gptr, T.data_ptr(), orth.data_ptr(), ref.data_ptr(), ms, None, 0, scratch.data_ptr(),
+              stream)
+    part = torch.empty(_lib.lib().dqz_absorb_split_scratch_bytes(L.n_nodes), dtype=torch.uint8, device=T.device)
+    out = torch.full_like(T, 7.0)
+    _lib.call("dqz_absorb_split", L.gptr, T.data_ptr(), orth.data_ptr(), out.data_ptr(), L.max_slice(), None, 0,
+              part.data_ptr(), stream)
+    for v in range(L.n_nodes):
+        o, n = int(L.node_off[v]), int(L.node_sizes()[v])
+        assert rel_err(out[o:o + n], ref[o:o + n]) < 1e-14, v
+    nodes = np.sort(rng.choice(L.n_nodes, L.n_nodes // 2, replace=False)).astype(np.int32)
+    out2 = torch.full_like(T, 7.0)
+    _lib.call("dqz_absorb_split", L.gptr, T.data_ptr(), orth.data_ptr(), out2.data_ptr(), L.max_slice(),
+              torch.from_numpy(nodes).cuda().data_ptr(), len(nodes), part.data_ptr(), stream)
+    for v in range(L.n_nodes):
+        o, n = int(L.node_off[v]), int(L.node_sizes()[v])
+        if v in nodes:
+            assert torch.equal(out2[o:o + n], out[o:o + n])
+        else:
+            assert bool((out2[o:o + n] == 7.0).all())
 
 
 @pytest.mark.parametrize("chi", [8, 16])
