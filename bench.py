@@ -694,6 +694,27 @@ def run_ours(args, world, rank, local):
     print(json.dumps(line), flush=True)
 
 
+def profile_hook(spec):
+    """``--profile-steps A:B`` -> a callable(step) that opens the CUDA
+    profiler range before step A and closes it before step B (for
+    ``ncu --profile-from-start off`` captures of a few steps); None without."""
+    if not spec:
+        return None
+    import torch
+
+    a, b = (int(x) for x in spec.split(":"))
+
+    def hook(step):
+        if step == a:
+            torch.cuda.synchronize()
+            torch.cuda.cudart().cudaProfilerStart()
+        elif step == b:
+            torch.cuda.synchronize()
+            torch.cuda.cudart().cudaProfilerStop()
+
+    return hook
+
+
 def run_anneal(args, world, rank, local):
     """Batched annealing: ``--instances`` random 3-regular instances with n
     uniform in [100, 1000] (even), J = +-1, h = 0, all advanced together by
@@ -729,10 +750,15 @@ def run_anneal(args, world, rank, local):
     with ClockSampler(local) as clk:
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        for _ in range(args.steps):
+        hook = profile_hook(args.profile_steps)
+        for i in range(args.steps):
+            if hook:
+                hook(i)
             s = s_of[t % n_steps]
             ba.step(-dt * (1 - s), dt * s, first=False, second_order=True)
             t += 1
+        if hook:
+            hook(args.steps)
         e1.record()
         e1.synchronize()
     elapsed = reduce_max(e0.elapsed_time(e1) * 1e-3, world)
@@ -881,14 +907,15 @@ def run_eagle(args, world, rank, local):
 
     from dequantizer_b200.workloads import run_eagle_simulation
 
-    n_steps = 20
+    n_steps = args.eagle_steps
     torch.cuda.synchronize()
     barrier(world)
     with ClockSampler(local) as clk:
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
         z, em = run_eagle_simulation(max_chi=32, layers_per_regauging=1, trotter_steps=n_steps, accuracy=1e-5,
-                                     theta=0.6, is_infinite=False, colour_classes=True, all_qubits=True)
+                                     theta=0.6, is_infinite=False, colour_classes=True, all_qubits=True,
+                                     on_step=profile_hook(args.profile_steps))
         e1.record()
         e1.synchronize()
     elapsed = reduce_max(e0.elapsed_time(e1) * 1e-3, world)
@@ -919,6 +946,10 @@ def main():
     ap.add_argument("--anneal-precision", choices=["fp64", "mixed"], default="fp64",
                     help="batched annealing: plain FP64, or BF16 tensor-core regauge sweeps handing over to FP64")
     ap.add_argument("--trotter-steps", type=int, default=200)
+    ap.add_argument("--eagle-steps", type=int, default=20, help="Trotter steps of the eagle workload")
+    ap.add_argument("--profile-steps", default=None,
+                    help="A:B -- CUDA profiler range over the timed steps A..B-1 of the anneal and eagle "
+                         "workloads (for ncu --profile-from-start off)")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)

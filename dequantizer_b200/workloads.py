@@ -16,7 +16,7 @@
 """
 
 from dataclasses import dataclass, field
-from typing import Dict, Iterable, List, Optional, Sequence, Tuple
+from typing import Callable, Dict, Iterable, List, Optional, Sequence, Tuple
 
 import numpy as np
 import torch
@@ -106,11 +106,13 @@ def run_eagle_simulation(
     traversal_type: str = "dfs",
     colour_classes: bool = False,
     all_qubits: bool = False,
+    on_step: Optional[Callable[[int], None]] = None,
 ):
     """Kicked-Ising dynamics; returns the target qubit's <Z> per layer (layer 0
     first), or every qubit's <Z> per layer when ``all_qubits``. With
     ``colour_classes`` the RZZ gates are applied class by class of a proper
-    edge colouring with a regauge after each class."""
+    edge colouring with a regauge after each class. ``on_step(t)`` is called
+    before Trotter step t and with t = trotter_steps after the last one."""
     lattice = get_heavy_hex_ibm_eagle_lattice_infinite() if is_infinite else get_heavy_hex_ibm_eagle_lattice()
     traverser = list(lattice.get_traversal_iterator())
     target = 2 if is_infinite else 62
@@ -128,7 +130,9 @@ def run_eagle_simulation(
         return float((rho[0, 0] - rho[1, 1]).real)
 
     out = [readout()]
-    for _ in range(trotter_steps):
+    for t in range(trotter_steps):
+        if on_step is not None:
+            on_step(t)
         for node_id in range(lattice.nodes_number):
             em.apply_q1(rx, node_id)
         if classes:
@@ -142,6 +146,8 @@ def run_eagle_simulation(
                 if isinstance(el, Edge):
                     em.apply_q2(rzz, el.id[0], el.id[1])
         out.append(readout())
+    if on_step is not None:
+        on_step(trotter_steps)
     return out, em
 
 
