@@ -42,9 +42,19 @@ __device__ __forceinline__ void node_slice_column(const dqz_graph_t &g, const cd
   const long long Re = s.stride[e];
   const long long P = s.size / ce;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  for (long long x = threadIdx.x; x < P; x += blockDim.x) {
-    long long l = x / Re, r = x - l * Re;
-    bufA[x] = Tv[(l * ce + a) * Re + r];
+  // P < 2^31 for every slice held on chip: the division by Re via FastDiv
+  const bool small = P * ce < (1ll << 31);
+  const FastDiv fRe((unsigned)(small ? Re : 1));
+  if (small) {
+    for (unsigned x = threadIdx.x; x < (unsigned)P; x += blockDim.x) {
+      const unsigned l = fRe.div(x), r = x - l * (unsigned)Re;
+      bufA[x] = Tv[(l * (unsigned)ce + (unsigned)a) * (unsigned)Re + r];
+    }
+  } else {
+    for (long long x = threadIdx.x; x < P; x += blockDim.x) {
+      long long l = x / Re, r = x - l * Re;
+      bufA[x] = Tv[(l * ce + a) * Re + r];
+    }
   }
   __syncthreads();
   cd *cur = bufA, *nxt = bufB;
@@ -63,9 +73,16 @@ __device__ __forceinline__ void node_slice_column(const dqz_graph_t &g, const cd
   }
   for (int ap = warp; ap < ce; ap += nw) {
     cd acc = czero();
-    for (long long x = lane; x < P; x += 32) {
-      long long l = x / Re, r = x - l * Re;
-      cfmac(acc, Tv[(l * ce + ap) * Re + r], cur[x]);
+    if (small) {
+      for (unsigned x = lane; x < (unsigned)P; x += 32) {
+        const unsigned l = fRe.div(x), r = x - l * (unsigned)Re;
+        cfmac(acc, Tv[(l * (unsigned)ce + (unsigned)ap) * (unsigned)Re + r], cur[x]);
+      }
+    } else {
+      for (long long x = lane; x < P; x += 32) {
+        long long l = x / Re, r = x - l * Re;
+        cfmac(acc, Tv[(l * ce + ap) * Re + r], cur[x]);
+      }
     }
     acc = warp_csum(acc);
     if (lane == 0) put(ap, acc);

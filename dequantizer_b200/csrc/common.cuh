@@ -117,6 +117,23 @@ __device__ __forceinline__ void load_shape(const dqz_graph_t &g, int v, NodeShap
   s.size = st;
 }
 
+// Division by a loop-invariant 32-bit divisor d >= 1 through a multiply-high,
+// the round-up method of Granlund and Montgomery ("Division by invariant
+// integers using multiplication", PLDI 1994): s = ceil(log2 d),
+// m = floor(2^32 (2^s - d) / d) + 1 (< 2^32), x / d = (umulhi(x, m) + x) >> s
+// for every 32-bit x. A hardware-free integer division costs a long
+// instruction sequence; this one a multiply-high, an add and a shift.
+struct FastDiv {
+  unsigned d, m, s;
+  __device__ __forceinline__ explicit FastDiv(unsigned dv) : d(dv) {
+    s = dv > 1 ? 32u - (unsigned)__clz(dv - 1u) : 0u;
+    m = (unsigned)((((1ull << 32) * ((1ull << s) - dv)) / dv) + 1ull);
+  }
+  __device__ __forceinline__ unsigned div(unsigned x) const {
+    return (unsigned)(((unsigned long long)__umulhi(x, m) + x) >> s);
+  }
+};
+
 // Generic CTA-cooperative mode product on a row-major tensor:
 //   Y[l, i, r] = sum_b M(i, b) X[l, b, r],  M(i, b) = m[i * rs + b * cs] (optionally conj)
 // X has shape (L, qin, R); Y has shape (L, qout, R). X and Y must not alias.
@@ -144,12 +161,36 @@ __device__ __forceinline__ void mode_product_idx(const cd *__restrict__ X, cd *_
   }
 }
 
+// The same with 32-bit indices and the divisions by R and qout through FastDiv
+// (total < 2^31).
+template <bool CONJ>
+__device__ __forceinline__ void mode_product_fast(const cd *__restrict__ X, cd *__restrict__ Y, unsigned L, int qin,
+                                                  int qout, unsigned R, const cd *__restrict__ m, int rs, int cs) {
+  const unsigned total = L * (unsigned)qout * R;
+  const FastDiv fR(R), fq((unsigned)qout);
+  for (unsigned o = threadIdx.x; o < total; o += blockDim.x) {
+    const unsigned t = fR.div(o);
+    const unsigned r = o - t * R;
+    const unsigned l = fq.div(t);
+    const int i = (int)(t - l * (unsigned)qout);
+    const cd *x = X + (l * (unsigned)qin) * R + r;
+    const cd *mm = m + (long long)i * rs;
+    cd acc = czero();
+    for (int b = 0; b < qin; ++b) {
+      cd mv = mm[(long long)b * cs];
+      if (CONJ) mv = cconj(mv);
+      cfma(acc, mv, x[(long long)b * R]);
+    }
+    Y[o] = acc;
+  }
+}
+
 template <bool CONJ>
 __device__ __forceinline__ void mode_product(const cd *__restrict__ X, cd *__restrict__ Y, long long L, int qin,
                                              int qout, long long R, const cd *__restrict__ m, int rs, int cs) {
   const long long big = (qin > qout ? qin : qout);
   if (L * big * R < (1ll << 31))
-    mode_product_idx<CONJ, int>(X, Y, (int)L, qin, qout, (int)R, m, rs, cs);
+    mode_product_fast<CONJ>(X, Y, (unsigned)L, qin, qout, (unsigned)R, m, rs, cs);
   else
     mode_product_idx<CONJ, long long>(X, Y, L, qin, qout, R, m, rs, cs);
 }
