@@ -427,11 +427,14 @@ constexpr size_t SUF_SMEM_MAX = 220 * 1024;  // dynamic shared memory per CTA (p
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(SUF_THREADS, 1)
     simple_update_onchip_kernel(dqz_graph_t g, cd *Tall, double *lambdas, const int32_t *edges,
                                 const uint8_t *ctrl_first, const cd *halves, const int32_t *ranks, int n, double eps,
-                                int max_rank, double *err_out, double *ent_out, long long cap, uint8_t *done) {
+                                int max_rank, double *err_out, double *ent_out, long long cap, uint8_t *done,
+                                cd *gws, int chained) {
   namespace cg = cooperative_groups;
   cg::cluster_group cluster = cg::this_cluster();
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  cd *sm = reinterpret_cast<cd *>(smem_raw);
+  // the side's matrices: in shared memory, or (gws) in this CTA's slice of a
+  // global workspace of `cap` entries per CTA, for jobs above shared memory
+  cd *sm = gws ? gws + (long long)blockIdx.x * cap : reinterpret_cast<cd *>(smem_raw);
   __shared__ double red[48];
   __shared__ int flag[4];
   __shared__ double sv[DQZ_MAX_CHI], lam_sh[DQZ_MAX_CHI], lam_in[DQZ_MAX_CHI];
@@ -452,8 +455,11 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(SUF_THREADS, 1)
     // decided on the job's shapes before any update; the mark tells the
     // global-scratch kernel (launched next) which jobs are done, since this
     // launch changes the bond dimensions the decision reads
+    // chained: a launch before this one marked the jobs it did (their shapes
+    // have changed since); the others are decided here and marked when done
+    if (chained && done[j]) continue;
     const bool fits = suf_fits(U, V, r, max_rank, cap);
-    if (side == 0 && threadIdx.x == 0) done[j] = fits ? 1 : 0;
+    if (side == 0 && threadIdx.x == 0 && (fits || !chained)) done[j] = fits ? 1 : 0;
     if (!fits) continue;  // left to the global-scratch kernel; same decision in both CTAs
     const SUSide &X = side ? V : U;
     SufDims D, Du, Dv;
@@ -518,9 +524,16 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(SUF_THREADS, 1)
     householder_qr_owned(Sm, D.MS, D.KS, tauS);
 
     // ---- swap R_S: the partner's R (muS x K, upper trapezoidal) into W, then the core
+    if (gws) __threadfence();
     cluster.sync();
     const SufDims &Dp = side ? Du : Dv;
-    {
+    if (gws) {  // the partner's workspace slice, read past L1
+      const cd *Sp = gws + (long long)(blockIdx.x ^ 1u) * cap;
+      for (int idx = tid; idx < Dp.muS * K; idx += nt) {
+        const int i = idx % Dp.muS, c = idx / Dp.muS;
+        W[idx] = c >= i ? __ldcg(Sp + i + (long long)c * Dp.MS) : czero();
+      }
+    } else {
       const cd *Sp = cluster.map_shared_rank(Sm, side ^ 1);
       for (int idx = tid; idx < Dp.muS * K; idx += nt) {
         const int i = idx % Dp.muS, c = idx / Dp.muS;
@@ -717,9 +730,23 @@ extern "C" int dqz_apply_half_gates(const void *tensors_in, void *tensors_out, c
 // kernel.
 __host__ __device__ inline size_t su_marks_bytes(int32_t n) { return ((size_t)n + 255) & ~(size_t)255; }
 
+// The cluster form with a global workspace (jobs above shared memory): at most
+// SU_CLUSTER_PAIRS jobs in flight (one CTA per SM), each CTA's slice bounded
+// by the side's need for matrices of max_rows x max_cols (B and S at most
+// max_rows x max_cols each, core / W / X at most 3 max_cols^2 beyond that).
+constexpr int SU_CLUSTER_PAIRS = 74;
+__host__ __device__ inline long long su_cluster_cap(int max_rows, int max_cols) {
+  return suf_even(2ll * max_rows * max_cols + 3ll * max_cols * max_cols + 8ll * max_cols + 64);
+}
+inline int su_cluster_pairs(int n) { return n < SU_CLUSTER_PAIRS ? n : SU_CLUSTER_PAIRS; }
+
 extern "C" size_t dqz_simple_update_scratch_bytes(int32_t n, int32_t max_rows, int32_t max_cols) {
   int grid = n < SU_GRID_MAX ? n : SU_GRID_MAX;
-  return su_marks_bytes(n) + (size_t)grid * su_scratch_per_job(max_rows, max_cols);
+  const size_t one_cta = (size_t)grid * su_scratch_per_job(max_rows, max_cols);
+  const size_t cluster = (max_rows >= SUF_MIN_ROWS && n > 0)
+                             ? (size_t)2 * su_cluster_pairs(n) * su_cluster_cap(max_rows, max_cols) * sizeof(cd)
+                             : 0;
+  return su_marks_bytes(n) + (one_cta > cluster ? one_cta : cluster);
 }
 
 extern "C" int dqz_simple_update(const dqz_graph_t *g, void *tensors, double *lambdas, const int32_t *edges,
@@ -744,16 +771,29 @@ extern "C" int dqz_simple_update(const dqz_graph_t *g, void *tensors, double *la
   // The on-chip form finishes a job sooner; the one-CTA kernel, several jobs
   // per SM, has more throughput on large batches (measured at bond 16: 440
   // jobs in 5.2 ms on chip, 4.4 ms on the one-CTA kernel; 112 jobs in 2.0 vs
-  // 3.3 ms). Batches of up to one job per SM take the on-chip form.
-  if (max_rows >= SUF_MIN_ROWS && n <= sms && dqz_get_tuning(DQZ_TUNE_SU_ONCHIP) != 1) {
+  // 3.3 ms). Batches of up to one job per SM take the on-chip form; the jobs
+  // of such a batch above shared memory (bond 32 between degree-3 nodes: a
+  // 1024 x 64 B per side) then take the same cluster form with its matrices
+  // in a global workspace (both sides at once, the two-step QR), the rest the
+  // one-CTA kernel. Knob DQZ_TUNE_SU_ONCHIP: 1 = the one-CTA kernel only,
+  // 2 = the cluster forms at any batch size, 3 = no global-workspace form.
+  const int knob = dqz_get_tuning(DQZ_TUNE_SU_ONCHIP);
+  const int pairs = n < sms / 2 ? n : sms / 2;  // one CTA per SM, two per cluster
+  if (max_rows >= SUF_MIN_ROWS && (n <= sms || knob == 2) && knob != 1) {
     DQZ_SMEM_ATTR_ONCE(simple_update_onchip_kernel, SUF_SMEM_MAX);
     const long long cap = (long long)(SUF_SMEM_MAX / sizeof(cd));
     marks = static_cast<uint8_t *>(scratch);
-    const int pairs = n < sms / 2 ? n : sms / 2;  // one CTA per SM, two per cluster
     simple_update_onchip_kernel<<<2 * pairs, SUF_THREADS, SUF_SMEM_MAX, stream>>>(
         *g, (cd *)tensors, lambdas, edges, ctrl_is_first, (const cd *)halves, ranks, n, eps, max_rank, err, entropy,
-        cap, marks);
+        cap, marks, nullptr, 0);
     DQZ_CHECK_LAUNCH();
+    if (knob != 3) {
+      const int cp = su_cluster_pairs(n) < pairs ? su_cluster_pairs(n) : pairs;
+      simple_update_onchip_kernel<<<2 * cp, SUF_THREADS, 0, stream>>>(
+          *g, (cd *)tensors, lambdas, edges, ctrl_is_first, (const cd *)halves, ranks, n, eps, max_rank, err,
+          entropy, su_cluster_cap(max_rows, max_cols), marks, job_scratch, 1);
+      DQZ_CHECK_LAUNCH();
+    }
   }
   DQZ_SMEM_ATTR_ONCE(simple_update_kernel, SMEM_LIMIT);
   int grid = n < SU_GRID_MAX ? n : SU_GRID_MAX;

@@ -78,7 +78,9 @@ int dqz_device_supported(int device); /* 1 when the device is sm_100 */
 #define DQZ_TUNE_GAUGE_DIST_WARPS 1 /* warps per CTA of the one-warp vidal_distance kernel (1..8) */
 #define DQZ_TUNE_GAUGE_PATH 2       /* 1: one-warp gauge kernels where they apply, 2: one CTA per item */
 #define DQZ_TUNE_SU_GRID 3          /* CTAs of simple_update (>= 1), jobs loop over the grid     */
-#define DQZ_TUNE_SU_ONCHIP 4        /* 1: every simple-update job on the global-scratch kernel      */
+#define DQZ_TUNE_SU_ONCHIP 4        /* simple update: 1 = one-CTA global-scratch kernel only,
+                                       2 = cluster forms at any batch size, 3 = no global-workspace
+                                       cluster form                                               */
 #define DQZ_TUNE_COUNT 5
 int dqz_set_tuning(int32_t knob, int32_t value); /* DQZ_ERR_ARG for an unknown knob or value < 0 */
 int32_t dqz_get_tuning(int32_t knob);            /* -1 for an unknown knob */
@@ -331,13 +333,15 @@ int dqz_apply_half_gates(const void *tensors_in, void *tensors_out, const int64_
  * Writes Gamma tensors in place (capacity layout), lambdas, edge_chi, and
  * err/entropy per job. max_rows / max_cols bound the rows (d x the other
  * bonds) and columns (bond x gate rank) of the jobs' matrices.
- * In batches of at most one job per SM, jobs with a 256-row matrix or more run,
- * where their matrices fit in shared memory, on an on-chip form (a cluster of
- * two CTAs per job, one per side: lower latency);
- * the others on a one-CTA kernel with its matrices in `scratch`. The scratch
- * (dqz_simple_update_scratch_bytes) also holds one byte per job recording
- * which form did it. Knob DQZ_TUNE_SU_ONCHIP = 1 sends every job to the
- * one-CTA kernel. Results agree to rounding and singular-vector phases. */
+ * In batches of at most one job per SM, jobs with a 256-row matrix or more run
+ * on a cluster form (two CTAs per job, one per side, a two-step QR: lower
+ * latency) with their matrices in shared memory where they fit, else in a
+ * global workspace inside `scratch`; the others on a one-CTA kernel with its
+ * matrices in `scratch`. The scratch (dqz_simple_update_scratch_bytes) also
+ * holds one byte per job recording which form did it. Knob
+ * DQZ_TUNE_SU_ONCHIP: 1 sends every job to the one-CTA kernel, 2 uses the
+ * cluster forms at any batch size, 3 keeps the global-workspace cluster form
+ * off. Results agree to rounding and singular-vector phases. */
 int dqz_simple_update(const dqz_graph_t *g, void *tensors, double *lambdas,
                       const int32_t *edges, const uint8_t *ctrl_is_first, const void *halves,
                       const int32_t *ranks, int32_t n, double eps, int32_t max_rank,

@@ -228,3 +228,76 @@ def test_batched_annealer_matches_oracle_per_instance(max_chi, sizes):
         assert np.abs(errs_b[k] - errs).max() < 1e-9
         reached, truncated = max(reached, max(bonds)), max(truncated, float(errs.max()))
     assert reached == max_chi and truncated > 1e-6
+
+
+@pytest.mark.parametrize("chi,nn", [(16, 600), (32, 96)])
+def test_simple_update_forms_agree_on_a_batch(chi, nn):
+    """One dqz_simple_update batch of node-disjoint bond-16 jobs (more jobs
+    than SMs) and of bond-32 jobs (2048 x 64 per side, above shared memory)
+    through each form the knob selects: the one-CTA global-scratch kernel
+    (su_onchip = 1), the cluster forms at any batch size (2), the default rule
+    (0) and the default without the global-workspace cluster form (3). Lambdas,
+    truncation errors and entropies agree to 1e-12, and the two-site tensors
+    around the updated bonds (gauge-invariant) to 1e-10 relative."""
+    from dequantizer_b200 import _lib, autotune
+    from dequantizer_b200.gates import decompose_gates
+    from dequantizer_b200.layout import GraphLayout
+
+    g = G.get_random_regular_graph(nn, 3, 2, chi, 1)
+    nodes, edges = list(g.nodes.values()), list(g.edges.values())
+    L = GraphLayout(nodes, edges, [chi] * len(edges))
+    rng = np.random.default_rng(chi)
+    T0 = L.new_tensor_arena()
+    z = rng.standard_normal((T0.numel(), 2))
+    T0.copy_(torch.from_numpy(z[:, 0] + 1j * z[:, 1]))
+    lam0 = L.new_lam_arena()
+    lam0.copy_(torch.from_numpy(np.concatenate([np.sort(10 ** rng.uniform(-3, 0, chi))[::-1]
+                                                for _ in range(L.n_edges)])))
+    taken, jobs = set(), []
+    for e in range(L.n_edges):
+        a, b = int(L.half_node[L.edge_half[2 * e]]), int(L.half_node[L.edge_half[2 * e + 1]])
+        if a not in taken and b not in taken:
+            taken |= {a, b}
+            jobs.append(e)
+    n = len(jobs)
+    gates = np.zeros((n, 4, 4), complex)
+    gates[:, range(4), range(4)] = np.exp(1j * rng.uniform(-3, 3, (n, 4)))
+    flat, ranks, _ = decompose_gates(gates.reshape(n, 2, 2, 2, 2), 1e-10)
+    rows, cols = 2 * chi * chi, chi * int(ranks.max())
+    dev = torch.device("cuda", 0)
+    ed = torch.tensor(jobs, dtype=torch.int32, device=dev)
+    first = torch.ones(n, dtype=torch.uint8, device=dev)
+    halves = torch.from_numpy(flat.reshape(n, -1)).to(dev)
+    rk = torch.from_numpy(ranks).to(dev)
+    out = {}
+    try:
+        for knob in (1, 2, 0, 3):
+            autotune.set_knobs({"su_onchip": knob})
+            T, lam = T0.clone(), lam0.clone()
+            err = torch.empty(n, dtype=torch.float64, device=dev)
+            ent = torch.empty_like(err)
+            scratch = torch.empty(_lib.lib().dqz_simple_update_scratch_bytes(n, rows, cols), dtype=torch.uint8,
+                                  device=dev)
+            _lib.call("dqz_simple_update", L.gptr, T.data_ptr(), lam.data_ptr(), ed.data_ptr(), first.data_ptr(),
+                      halves.data_ptr(), rk.data_ptr(), n, 1e-10, chi, rows, cols, err.data_ptr(), ent.data_ptr(),
+                      scratch.data_ptr(), _lib.stream_handle())
+            torch.cuda.synchronize()
+            L.edge_chi[:] = chi  # max_rank = chi keeps every bond at chi
+            L.push_edge_chi()
+            out[knob] = (T, lam, err, ent)
+    finally:
+        autotune.set_knobs({"su_onchip": 0})
+    ref = out[1]
+    for knob in (2, 0, 3):
+        T, lam, err, ent = out[knob]
+        assert float((lam - ref[1]).abs().max()) < 1e-12
+        assert float((err - ref[2]).abs().max()) < 1e-12
+        assert float((ent - ref[3]).abs().max()) < 1e-12
+        ta, tr = L.unpack_tensors(T), L.unpack_tensors(ref[0])
+        for e in jobs[:: max(1, n // 8)]:
+            ha, hb = int(L.edge_half[2 * e]), int(L.edge_half[2 * e + 1])
+            a, b = int(L.half_node[ha]), int(L.half_node[hb])
+            ia, ib = ha - int(L.node_half[a]), hb - int(L.node_half[b])
+            got = two_site(ta[a], ta[b], ia, ib, L.lambda_view(lam, e))
+            want = two_site(tr[a], tr[b], ia, ib, L.lambda_view(ref[1], e))
+            assert rel_err(got, want) < 1e-10

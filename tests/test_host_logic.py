@@ -43,7 +43,13 @@ def test_scratch_queries_are_host_only():
     assert lib.dqz_bp_node_scratch_bytes(100, 65536, 32) > 0
     # one byte per job (rounded up to 256) marking the on-chip jobs, then a
     # 64 * rows * cols slice per CTA of the global-scratch kernel
-    assert lib.dqz_simple_update_scratch_bytes(10, 2048, 64) == 256 + 10 * 64 * 2048 * 64
+    # marks, then the larger of the one-CTA kernel's matrices (4 x rows x cols
+    # complex per job) and the cluster form's global workspace (two CTAs per
+    # job, 2 rows cols + 3 cols^2 + 8 cols + 64 complex each)
+    one_cta = 10 * 64 * 2048 * 64
+    cluster = 2 * 10 * (2 * 2048 * 64 + 3 * 64 * 64 + 8 * 64 + 64) * 16
+    assert lib.dqz_simple_update_scratch_bytes(10, 2048, 64) == 256 + max(one_cta, cluster)
+    assert lib.dqz_simple_update_scratch_bytes(10, 128, 16) == 256 + 10 * 64 * 128 * 16
     assert lib.dqz_absorb_scratch_bytes(127, 8192) > 0
 
 
