@@ -552,7 +552,8 @@ def workload_suite(args):
                         "bf16_sweeps_per_regauge": (float(np.mean(ba.bf16_sweeps[b0:])) if ba.bf16_sweeps[b0:]
                                                     else 0.0),
                         "fp32_sweeps_per_regauge": (float(np.mean(ba.fp32_sweeps[b0:])) if ba.fp32_sweeps[b0:]
-                                                    else 0.0)}
+                                                    else 0.0),
+                        "gauge_evaluations_per_regauge": float(np.mean(ba.vd_checks[n0:]))}
         del ba
         torch.cuda.empty_cache()
     anneal["mixed_over_fp64"] = anneal["mixed"]["value"] / anneal["fp64"]["value"]

@@ -23,6 +23,7 @@ min(max_chi, rank bounds), evaluated for a whole level with numpy.
 """
 
 import logging
+import math
 from typing import List, Optional, Sequence
 
 import numpy as np
@@ -69,12 +70,15 @@ class BatchedAnnealer:
         ``bf16_max_sweeps``), then FP32 sweeps (dqz_bp_node_update_k3,
         complex64) until it falls to ``fp32_handover`` (at most
         ``fp32_max_sweeps``; BF16 products settle near 5e-5, FP32 ones near
-        1e-7); the FP64 loop of the reference (sweep, Vidal gauge, Vidal
-        distance until the accuracy) then finishes from there, normally after
-        one pass, since the gauge and distance evaluations of the sweeps in
-        between are skipped. Eigen and singular value decompositions, the
-        distances and the gates stay FP64. ``precision="fp64"`` is the plain
-        form."""
+        1e-7); FP64 sweeps then finish from there to the reference's stopping
+        rule (Vidal distance at most the accuracy, FP64 gauge and distance),
+        but the gauge and distance are evaluated after the first two sweeps
+        and then only when the geometric rate of the last two evaluations
+        predicts the accuracy (at most 8 sweeps apart), not after every sweep:
+        an instance stops at or a few sweeps past the reference's stopping
+        point. Eigen and singular value decompositions, the distances and the
+        gates stay FP64. ``precision="fp64"`` is the plain form (the
+        reference's loop exactly)."""
         if schedule not in ("sync", "flooding"):
             raise ValueError("batched annealing runs the synchronous or flooding BP schedule")
         if precision not in ("fp64", "mixed"):
@@ -86,6 +90,7 @@ class BatchedAnnealer:
         self.fp32_max_sweeps = int(fp32_max_sweeps)
         self.bf16_sweeps: List[List[int]] = []
         self.fp32_sweeps: List[List[int]] = []
+        self.vd_checks: List[List[int]] = []
         if not torch.cuda.is_available():
             raise RuntimeError("BatchedAnnealer runs on the GPU only")
         _lib.lib()
@@ -247,6 +252,10 @@ class BatchedAnnealer:
                 todo &= self.max_iters > 0
             if todo.any():
                 n2e, e2n = self._bf16_prephase(T, n2e, e2n, todo)
+        lazy = self.precision == "mixed"
+        next_check = np.ones(self.n_inst, dtype=np.int64)
+        hist: List[List] = [[] for _ in range(self.n_inst)]
+        checks = np.zeros(self.n_inst, dtype=np.int64)
         while True:
             active = vd_h > self.accuracy
             if self.max_iters is not None:
@@ -256,20 +265,48 @@ class BatchedAnnealer:
                 active &= iters < self.max_iters
             if not active.any():
                 break
-            every = bool(active.all())
             halves = torch.from_numpy(self._ranges(self.half_bounds, active)).to(dev)
-            edges = None if every else torch.from_numpy(self._ranges(self.edge_bounds, active)).to(dev)
-            nodes = None if every else torch.from_numpy(self._ranges(self.node_bounds, active)).to(dev)
             n2e_new, e2n_new = n2e.clone(), torch.empty_like(e2n)
             self._sweep_halves(T, n2e, e2n, n2e_new, e2n_new, halves)
             n2e, e2n = n2e_new, e2n_new
+            iters += active
+            # the Vidal gauge and distance: after every sweep (the reference's
+            # loop), or in the mixed form when the instance's distance is
+            # predicted to reach the accuracy (or at the iteration cap)
+            due = active & (iters >= next_check) if lazy else active
+            if lazy and self.max_iters is not None:
+                due |= active & (iters >= self.max_iters)
+            if not due.any():
+                continue
+            every = bool(due.all())
+            halves = torch.from_numpy(self._ranges(self.half_bounds, due)).to(dev)
+            edges = None if every else torch.from_numpy(self._ranges(self.edge_bounds, due)).to(dev)
+            nodes = None if every else torch.from_numpy(self._ranges(self.node_bounds, due)).to(dev)
             vidal_gauge_packed(L, T, n2e, EPS, out=(G, lam, orth), edges=edges, nodes=nodes)
             vidal_distance_partial(L, G, lam, EPS, partial, halves=None if every else halves)
             vd_h = self._per_instance_vd(partial).cpu().numpy()
-            iters += active
+            checks += due
+            if lazy:
+                for k in np.nonzero(due)[0]:
+                    hist[k].append((int(iters[k]), float(vd_h[k])))
+                    next_check[k] = iters[k] + self._sweeps_to_accuracy(hist[k])
         self.bp_iterations.append(iters.tolist())
+        self.vd_checks.append(checks.tolist())
         self.vidal_distances.append(vd_h.copy())
         return G, lam
+
+    def _sweeps_to_accuracy(self, hist, max_gap: int = 8) -> int:
+        """FP64 sweeps until the next distance check of the mixed form: the
+        geometric rate of the last two checks extrapolated to the accuracy
+        (1 while fewer than two checks or no decrease, at most ``max_gap``)."""
+        if len(hist) < 2:
+            return 1
+        (i1, v1), (i2, v2) = hist[-2], hist[-1]
+        if not (0.0 < v2 < v1) or i2 <= i1 or v2 <= self.accuracy:
+            return 1
+        rate = (v2 / v1) ** (1.0 / (i2 - i1))
+        k = math.ceil(math.log(self.accuracy / v2) / math.log(rate))
+        return int(min(max(k, 1), max_gap))
 
     def _bf16_prephase(self, T, n2e, e2n, active: np.ndarray):
         """Low-precision sweeps of the listed instances (complex64 messages),
