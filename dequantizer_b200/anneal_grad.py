@@ -68,6 +68,22 @@ def safe_sqrt_truncate(x: torch.Tensor, eps: float) -> torch.Tensor:
     return torch.where(keep, torch.sqrt(torch.where(keep, x, torch.ones_like(x))), torch.zeros_like(x))
 
 
+def _clone(x):
+    """A detached copy of a state part (one tensor, or a list of them)."""
+    return x.clone() if isinstance(x, torch.Tensor) else [t.clone() for t in x]
+
+
+def _leaves(x):
+    """Leaf copies (requires_grad) of a checkpointed state part."""
+    if isinstance(x, torch.Tensor):
+        return x.clone().requires_grad_(True)
+    return [t.clone().requires_grad_(True) for t in x]
+
+
+def _parts(x) -> List[torch.Tensor]:
+    return [x] if isinstance(x, torch.Tensor) else list(x)
+
+
 def _bcast(vec: torch.Tensor, axis: int, ndim: int) -> torch.Tensor:
     shape = [1] * ndim
     shape[axis] = vec.shape[0]
@@ -122,6 +138,15 @@ class AnnealingGradient:
         self.gate_J = torch.tensor([g[5] for g in self.gates], dtype=torch.float64, device=self.device)
         self.gate_hu = torch.tensor([g[6] for g in self.gates], dtype=torch.float64, device=self.device)
         self.gate_hv = torch.tensor([g[7] for g in self.gates], dtype=torch.float64, device=self.device)
+        # stacked form: once every node has the same degree and every bond is
+        # at max_chi (shapes no longer change), the state is one tensor
+        # G (N, chi, .., chi, 2) and one L (E, chi), and every stage is a few
+        # batched operations instead of one per node (host-side dispatch and
+        # autograd bookkeeping dominated the per-node lists)
+        degs = {len(n.neighbors) for n in self.nodes}
+        self.uniform_degree = degs.pop() if len(degs) == 1 else 0
+        self._stk = None
+        self.use_stacked = True
 
     # ------------------------------------------------------------- state
     def initial_state(self) -> Tuple[List[torch.Tensor], List[torch.Tensor]]:
@@ -196,26 +221,17 @@ class AnnealingGradient:
         X = torch.movedim(X, 1, -1)
         return X
 
-    def _simple_update_group(self, gam, lam, idx: List[int], h1, h2):
-        """tensor_ops.py:318-389 for node-disjoint gates of identical shapes,
-        as one batch (rank = min(max_chi, available))."""
-        gts = [self.gates[j] for j in idx]
-        B = len(gts)
-
-        def side(node_pos, bond_pos, half):
-            X = torch.stack([torch.movedim(gam[g[node_pos]], g[bond_pos], 0) for g in gts])
-            nb = X.dim() - 2  # bonds of the node
-            others = []
-            for p in range(nb - 1):
-                others.append(torch.stack([lam[[f for q, f in enumerate(self.node_edges[g[node_pos]])
-                                                if q != g[bond_pos]][p]] for g in gts]))
-            P = self._prepare(X, others, half)
-            return P, others
-
-        Pa, oa = side(1, 2, h1)
-        Pb, ob = side(3, 4, h2)
+    def _su_core(self, Xa, oa, Xb, ob, lam_e, h1, h2):
+        """tensor_ops.py:318-389 for a batch of gates of identical shapes: Xa /
+        Xb (B, c_e, others.., d) with the gate bond first, oa / ob the lambdas of
+        the other bonds ((B, c) each, in bond order), lam_e (B, c_e) the gate
+        bond's. Returns the new Gammas (B, others.., d, rank), rank last, and
+        the kept lambdas (B, rank); rank = min(max_chi, available)."""
+        B = Xa.shape[0]
+        Pa = self._prepare(Xa, oa, h1)
+        Pb = self._prepare(Xb, ob, h2)
         K = Pa.shape[-1]
-        d = torch.stack([lam[g[0]] for g in gts]).repeat_interleave(h1.shape[1], dim=1).to(torch.complex128)
+        d = lam_e.repeat_interleave(h1.shape[1], dim=1).to(torch.complex128)
         Wa, S, Wb = product_svd(Pa.reshape(B, -1, K) * d.unsqueeze(1), Pb.reshape(B, -1, K))
         lmbd = (S > self.eps).to(S.dtype) * S
         rank = min(self.max_chi, S.shape[-1])
@@ -229,11 +245,28 @@ class AnnealingGradient:
                 q = q * safe_inverse(L, self.eps).reshape(shape).to(q.dtype)
             return q
 
-        qa = finish(Wa, Pa, oa)
-        qb = finish(Wb, Pb, ob)
+        return finish(Wa, Pa, oa), finish(Wb, Pb, ob), lmbd[:, :rank]
+
+    def _simple_update_group(self, gam, lam, idx: List[int], h1, h2):
+        """tensor_ops.py:318-389 for node-disjoint gates of identical shapes,
+        as one batch (rank = min(max_chi, available))."""
+        gts = [self.gates[j] for j in idx]
+
+        def side(node_pos, bond_pos):
+            X = torch.stack([torch.movedim(gam[g[node_pos]], g[bond_pos], 0) for g in gts])
+            nb = X.dim() - 2  # bonds of the node
+            others = []
+            for p in range(nb - 1):
+                others.append(torch.stack([lam[[f for q, f in enumerate(self.node_edges[g[node_pos]])
+                                                if q != g[bond_pos]][p]] for g in gts]))
+            return X, others
+
+        Xa, oa = side(1, 2)
+        Xb, ob = side(3, 4)
+        lam_e = torch.stack([lam[g[0]] for g in gts])
+        qa, qb, lk = self._su_core(Xa, oa, Xb, ob, lam_e, h1, h2)
         gam = list(gam)
         lam = list(lam)
-        lk = lmbd[:, :rank]
         for g, xa, xb, l in zip(gts, qa.unbind(0), qb.unbind(0), lk.unbind(0)):
             gam[g[1]] = torch.movedim(xa, xa.dim() - 1, g[2])  # (others.., d, rank): rank to the bond slot
             gam[g[3]] = torch.movedim(xb, xb.dim() - 1, g[4])
@@ -253,6 +286,121 @@ class AnnealingGradient:
                 h1, h2 = self.coupling_halves(tau, idx)
                 gam, lam = self._simple_update_group(gam, lam, idx, h1, h2)
         return gam, lam
+
+    # ------------------------------------------------------- stacked form
+    def _stacked_tables(self):
+        """Index tables of the stacked form (built once): node -> edges of its
+        bonds, edge ends as half-edges, the per-half-edge source of the
+        orthogonalisers, the coupling levels grouped by the gate's bond slots,
+        and the fixed-point problem with every bond at max_chi."""
+        if self._stk is not None:
+            return self._stk
+        dev, k, c = self.device, self.uniform_degree, self.max_chi
+        E = len(self.edges)
+        t = {"ne": torch.as_tensor(self.node_edges, dtype=torch.long, device=dev)}
+        hf = [a * k + ia for a, ia, _, _ in self.edge_ends]
+        hb = [b * k + ib for _, _, b, ib in self.edge_ends]
+        t["hf"] = torch.as_tensor(hf, dtype=torch.long, device=dev)
+        t["hb"] = torch.as_tensor(hb, dtype=torch.long, device=dev)
+        perm = np.zeros(len(self.nodes) * k, dtype=np.int64)
+        perm[hf] = np.arange(E)
+        perm[hb] = E + np.arange(E)
+        t["orth_src"] = torch.as_tensor(perm, device=dev)
+        levels = []
+        for level in self.levels:
+            groups = {}
+            for j in level:
+                groups.setdefault((self.gates[j][2], self.gates[j][4]), []).append(j)
+            out = []
+            for (ia, ib), js in groups.items():
+                gts = [self.gates[j] for j in js]
+
+                def others(node_pos, bond_pos):
+                    return torch.as_tensor([[f for q, f in enumerate(self.node_edges[g[node_pos]]) if q != g[bond_pos]]
+                                            for g in gts], dtype=torch.long, device=dev)
+
+                out.append({"gates": js, "ia": ia, "ib": ib,
+                            "a": torch.as_tensor([g[1] for g in gts], dtype=torch.long, device=dev),
+                            "b": torch.as_tensor([g[3] for g in gts], dtype=torch.long, device=dev),
+                            "e": torch.as_tensor([g[0] for g in gts], dtype=torch.long, device=dev),
+                            "oa": others(1, 2), "ob": others(3, 4)})
+            levels.append(out)
+        t["levels"] = levels
+        for e in self.edges:
+            e.dimension = c
+        t["problem"] = FixedPointProblem(self.graph, topo=self.topo)
+        L = t["problem"].layout
+        t["he"] = torch.as_tensor(L.half_edge.astype(np.int64), device=dev)
+        self._stk = t
+        return t
+
+    def _stackable(self, gam, lam) -> bool:
+        if not self.use_stacked or not self.uniform_degree or isinstance(gam, torch.Tensor):
+            return False
+        c, k = self.max_chi, self.uniform_degree
+        shape = (c,) * k + (2,)
+        return all(int(l.shape[0]) == c for l in lam) and all(tuple(g.shape) == shape for g in gam)
+
+    def _coupling_layer_stacked(self, G, L, tau):
+        """coupling_layer on the stacked form: per level, the gates grouped by
+        their bond slots, one batch each, written back with one index_copy."""
+        t = self._stacked_tables()
+        k = self.uniform_degree
+        for groups in t["levels"]:
+            idx, new, eidx, lnew = [], [], [], []
+            for grp in groups:
+                h1, h2 = self.coupling_halves(tau, grp["gates"])
+                ia, ib = grp["ia"], grp["ib"]
+                Xa = torch.movedim(G[grp["a"]], 1 + ia, 1)
+                Xb = torch.movedim(G[grp["b"]], 1 + ib, 1)
+                oa = [L[grp["oa"][:, p]] for p in range(k - 1)]
+                ob = [L[grp["ob"][:, p]] for p in range(k - 1)]
+                qa, qb, lk = self._su_core(Xa, oa, Xb, ob, L[grp["e"]], h1, h2)
+                idx += [grp["a"], grp["b"]]
+                new += [torch.movedim(qa, qa.dim() - 1, 1 + ia), torch.movedim(qb, qb.dim() - 1, 1 + ib)]
+                eidx.append(grp["e"])
+                lnew.append(lk)
+            G = G.index_copy(0, torch.cat(idx), torch.cat(new))
+            L = L.index_copy(0, torch.cat(eidx), torch.cat(lnew))
+        return G, L
+
+    def _regauge_stacked(self, G, L):
+        """regauge on the stacked form (same operations, batched over all
+        nodes and edges)."""
+        t = self._stacked_tables()
+        P = t["problem"]
+        lay = P.layout
+        N, k, c = G.shape[0], self.uniform_degree, self.max_chi
+        sl = safe_sqrt_truncate(L, self.eps)
+        X = G
+        for f in range(k):
+            shape = [N] + [1] * (k + 1)
+            shape[f + 1] = c
+            X = X * sl[t["ne"][:, f]].reshape(shape).to(X.dtype)
+        X = X / torch.linalg.vector_norm(X.reshape(N, -1), dim=1).reshape((-1,) + (1,) * (k + 1))
+        with torch.no_grad():
+            n2e0 = torch.zeros(max(lay.msg_elems, 1), dtype=torch.complex128, device=self.device)
+            n2e0[: lay.n_halves * c * c] = torch.diag_embed(L.detach().to(torch.complex128)[t["he"]]).reshape(-1)
+        T_arena = X.reshape(-1)
+        if T_arena.requires_grad:
+            n2e, _ = BPFixedPoint.apply(T_arena, P, n2e0, self.bp_tol, self.bp_max, self.bp_tol, self.bp_max)
+        else:
+            n2e, _, _ = P.converge(T_arena, n2e0, self.bp_tol, self.bp_max)
+        self.last_bp_sweeps.append(P.last_sweeps)
+        per_half = n2e[: lay.n_halves * c * c].view(lay.n_halves, c, c)
+        Gf, Gb, lb = self._edge_svd(per_half[t["hf"]], per_half[t["hb"]])
+        O = torch.cat([Gf, Gb])[t["orth_src"]].view(N, k, c, c)
+        ax = "abcdefgh"[:k]
+        out = "pqrstuvw"[:k]
+        spec = "n" + ax + "s," + ",".join("n" + ax[f] + out[f] for f in range(k)) + "->n" + out + "s"
+        X = torch.einsum(spec, X, *[O[:, f] for f in range(k)])
+        X = X / torch.linalg.vector_norm(X.reshape(N, -1), dim=1).reshape((-1,) + (1,) * (k + 1))
+        return X, lb
+
+    def _apply1_stacked(self, G, gate):
+        X = torch.tensordot(G, gate, dims=([G.dim() - 1], [1]))
+        N = X.shape[0]
+        return X / torch.linalg.vector_norm(X.reshape(N, -1), dim=1).reshape((-1,) + (1,) * (X.dim() - 1))
 
     def _problem(self, lam) -> FixedPointProblem:
         for e, l in zip(self.edges, lam):
@@ -368,15 +516,35 @@ class AnnealingGradient:
         return m_sq_inv_f @ u, m_sq_inv_b @ vh.mT, s
 
     def step(self, gam, lam, s_t, first: bool):
+        """One second-order step. The state is per-node / per-edge lists, or
+        (stacked form, from the first step whose input has every bond at
+        max_chi on a graph of uniform degree) one tensor each."""
         tau_m = -self.dt * (1.0 - s_t)
         tau_c = self.dt * s_t
+        if self._stackable(gam, lam):
+            gam, lam = torch.stack(list(gam)), torch.stack(list(lam))
+        half = self.mixing_gate(tau_m / 2)
+        if isinstance(gam, torch.Tensor):
+            if not first:
+                gam, lam = self._regauge_stacked(gam, lam)
+            gam = self._apply1_stacked(gam, half)
+            gam, lam = self._coupling_layer_stacked(gam, lam, tau_c)
+            return self._apply1_stacked(gam, half), lam
         if not first:
             gam, lam = self.regauge(gam, lam)
-        half = self.mixing_gate(tau_m / 2)
         gam = self.apply1_all(gam, half)
         gam, lam = self.coupling_layer(gam, lam, tau_c)
         gam = self.apply1_all(gam, half)
         return gam, lam
+
+    def final_regauge(self, gam, lam):
+        """The last regauge; returns per-node / per-edge lists."""
+        if self._stackable(gam, lam):
+            gam, lam = torch.stack(list(gam)), torch.stack(list(lam))
+        if isinstance(gam, torch.Tensor):
+            gam, lam = self._regauge_stacked(gam, lam)
+            return list(gam.unbind(0)), list(lam.unbind(0))
+        return self.regauge(gam, lam)
 
     # ------------------------------------------------------- observables
     def energy_of(self, gam, lam) -> torch.Tensor:
@@ -421,7 +589,7 @@ class AnnealingGradient:
         with torch.no_grad():
             for t in range(s.shape[0]):
                 gam, lam = self.step(gam, lam, s[t], first=(t == 0))
-            return self.regauge(gam, lam)
+            return self.final_regauge(gam, lam)
 
     def forward(self, s_values: torch.Tensor):
         """No-grad forward; returns (energy, checkpoints)."""
@@ -430,9 +598,9 @@ class AnnealingGradient:
         with torch.no_grad():
             for t in range(s_values.shape[0]):
                 if t % self.k == 0:
-                    checkpoints.append((t, [g.clone() for g in gam], [l.clone() for l in lam]))
+                    checkpoints.append((t, _clone(gam), _clone(lam)))
                 gam, lam = self.step(gam, lam, s_values[t], first=(t == 0))
-            gam, lam = self.regauge(gam, lam)
+            gam, lam = self.final_regauge(gam, lam)
             E = self.energy_of(gam, lam)
         return E, checkpoints
 
@@ -450,21 +618,22 @@ class AnnealingGradient:
         for ci in range(len(checkpoints) - 1, -1, -1):
             t0, g0, l0 = checkpoints[ci]
             t1 = checkpoints[ci + 1][0] if ci + 1 < len(checkpoints) else n
-            gam = [g.clone().requires_grad_(True) for g in g0]
-            lam = [l.clone().requires_grad_(True) for l in l0]
+            gam, lam = _leaves(g0), _leaves(l0)
             s_seg = s_all[t0:t1].clone().requires_grad_(True)
             g_cur, l_cur = gam, lam
             for j in range(t1 - t0):
                 g_cur, l_cur = self.step(g_cur, l_cur, s_seg[j], first=(t0 + j == 0))
             if cot is None:
-                g_cur, l_cur = self.regauge(g_cur, l_cur)
+                g_cur, l_cur = self.final_regauge(g_cur, l_cur)
                 outs = [self.energy_of(g_cur, l_cur)]
                 gouts = [torch.ones_like(outs[0])]
             else:
-                pairs = [(o, c) for o, c in zip(list(g_cur) + list(l_cur), cot) if o.requires_grad]
+                # this segment's output has the representation of the next
+                # segment's checkpoint (the same steps produced both)
+                pairs = [(o, c) for o, c in zip(_parts(g_cur) + _parts(l_cur), cot) if o.requires_grad]
                 outs = [o for o, _ in pairs]
                 gouts = [c for _, c in pairs]
-            ins = list(gam) + list(lam) + [s_seg]
+            ins = _parts(gam) + _parts(lam) + [s_seg]
             grads = torch.autograd.grad(outs, ins, grad_outputs=gouts, allow_unused=True)
             grads = [torch.zeros_like(x) if gr is None else gr for x, gr in zip(ins, grads)]
             grad[t0:t1] += grads[-1]
