@@ -739,11 +739,16 @@ def run_anneal(args, world, rank, local):
     s_of = [t / (n_steps - 1) for t in range(n_steps)]
     ba = BatchedAnnealer(energies, max_chi=args.chi, accuracy=1e-5, max_belief_propagation_iterations=100,
                          precision=args.anneal_precision)
+    if args.anneal_sample == "mid":
+        # the suite's sample: warm-up steps of a larger dt at s = 0.5 entangle
+        # the state (every bond at the cap), then steps of dt at s = 0.5
+        s_of = [0.5] * n_steps
     torch.cuda.synchronize()
     t = 0
     for _ in range(args.warmup):
         s = s_of[t % n_steps]
-        ba.step(-dt * (1 - s), dt * s, first=(t == 0), second_order=True)
+        dw = args.suite_anneal_warm_dt if args.anneal_sample == "mid" else dt
+        ba.step(-dw * (1 - s), dw * s, first=(t == 0), second_order=True)
         t += 1
     torch.cuda.synchronize()
     barrier(world)
@@ -777,6 +782,7 @@ def run_anneal(args, world, rank, local):
                        "trotter_steps": n_steps, "dt": dt, "order": 2, "bp_accuracy": 1e-5,
                        "bp_schedule": "synchronous, per-instance convergence"},
             "timed_s_range": [s_of[args.warmup % n_steps], s_of[(t - 1) % n_steps]],
+            "sample": args.anneal_sample,
             "bp_edge_updates_per_s_rank0": upd / elapsed,
             "bp_sweeps_per_regauge_rank0": {"mean": float(np.mean(ba.bp_iterations[sw0:])),
                                             "max": int(np.max(ba.bp_iterations[sw0:]))},
@@ -959,6 +965,9 @@ def main():
     ap.add_argument("--ref-seconds", type=float, default=4.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-suite", action="store_true", help="skip the bounded runs of the other workloads")
+    ap.add_argument("--anneal-sample", choices=["schedule", "mid"], default="schedule",
+                    help="anneal workload: steps along the schedule (default), or the suite's mid-schedule sample "
+                         "(warm-up steps of --suite-anneal-warm-dt at s = 0.5, then steps of dt at s = 0.5)")
     ap.add_argument("--suite-anneal-warmup", type=int, default=6)
     ap.add_argument("--suite-anneal-steps", type=int, default=4)
     ap.add_argument("--suite-anneal-warm-dt", type=float, default=1.0)
