@@ -20,7 +20,8 @@ import torch
 
 from . import _lib
 
-KNOBS = {"gauge_edge_warps": 0, "gauge_dist_warps": 1, "gauge_path": 2, "su_grid": 3, "su_onchip": 4}
+KNOBS = {"gauge_edge_warps": 0, "gauge_dist_warps": 1, "gauge_path": 2, "su_grid": 3, "su_onchip": 4,
+         "sweep_onecta": 5}
 
 
 def set_knobs(cfg: Dict[str, int]) -> None:

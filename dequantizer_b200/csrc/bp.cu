@@ -140,6 +140,114 @@ __global__ void __launch_bounds__(BP_THREADS) bp_node_generic(dqz_graph_t g, con
     node_update_half(g, T, n2e_old, e2n_old, n2e_new, src_sel, halves[item], out, bufA, bufB, trace_sh);
 }
 
+// ---- one warp per half-edge, for small nodes. The same elements in the same
+// order as node_update_half (each mode-product output by one lane, the final
+// column by the lanes' partial sums and warp_csum, the trace by one lane), so
+// the messages are bit-identical; phases are separated by __syncwarp only.
+__device__ __forceinline__ void warp_mode_product(const cd *__restrict__ X, cd *__restrict__ Y, unsigned L, int q,
+                                                  unsigned R, const cd *__restrict__ m) {
+  const unsigned total = L * (unsigned)q * R;
+  const FastDiv fR(R), fq((unsigned)q);
+  for (unsigned o = threadIdx.x & 31; o < total; o += 32) {
+    const unsigned t = fR.div(o);
+    const unsigned r = o - t * R;
+    const unsigned l = fq.div(t);
+    const int i = (int)(t - l * (unsigned)q);
+    const cd *x = X + (l * (unsigned)q) * R + r;
+    cd acc = czero();
+    for (int b = 0; b < q; ++b) cfma(acc, m[(long long)i * q + b], x[(long long)b * R]);
+    Y[o] = acc;
+  }
+}
+
+__device__ __forceinline__ void warp_node_update_half(const dqz_graph_t &g, const cd *__restrict__ T, const cd *n2e_old,
+                                                      const cd *e2n_old, cd *n2e_new,
+                                                      const uint8_t *__restrict__ src_sel, int h, cd *out, cd *bufA,
+                                                      cd *bufB) {
+  const int lane = threadIdx.x & 31;
+  const int v = g.half_node[h];
+  NodeShape s;
+  load_shape(g, v, s);
+  const int e = h - s.half0;
+  const int ce = s.dims[e];
+  const cd *Tv = T + g.node_off[v];
+  const unsigned Re = (unsigned)s.stride[e];
+  const unsigned P = (unsigned)(s.size / ce);
+  const FastDiv fRe(Re);
+  for (int a = 0; a < ce; ++a) {
+    for (unsigned x = lane; x < P; x += 32) {
+      const unsigned l = fRe.div(x), r = x - l * Re;
+      bufA[x] = Tv[(l * (unsigned)ce + (unsigned)a) * Re + r];
+    }
+    __syncwarp();
+    cd *cur = bufA, *nxt = bufB;
+    unsigned Lj = 1;
+    for (int f = 0; f < s.k; ++f) {
+      if (f == e) continue;
+      const int q = s.dims[f];
+      const unsigned R = P / Lj / (unsigned)q;
+      warp_mode_product(cur, nxt, Lj, q, R, incoming_msg(g, s.half0 + f, n2e_old, e2n_old, n2e_new, src_sel));
+      __syncwarp();
+      cd *t = cur;
+      cur = nxt;
+      nxt = t;
+      Lj *= (unsigned)q;
+    }
+    for (int ap = 0; ap < ce; ++ap) {
+      cd acc = czero();
+      for (unsigned x = lane; x < P; x += 32) {
+        const unsigned l = fRe.div(x), r = x - l * Re;
+        cfmac(acc, Tv[(l * (unsigned)ce + (unsigned)ap) * Re + r], cur[x]);
+      }
+      acc = warp_csum(acc);
+      if (lane == 0) out[ap * ce + a] = acc;
+    }
+    __syncwarp();
+  }
+  cd tr = czero();
+  if (lane == 0)
+    for (int i = 0; i < ce; ++i) tr = cadd(tr, out[i * ce + i]);
+  tr.x = __shfl_sync(0xffffffffu, tr.x, 0);
+  tr.y = __shfl_sync(0xffffffffu, tr.y, 0);
+  cd *dst = n2e_new + g.half_msg_off[h];
+  for (int i = lane; i < ce * ce; i += 32) dst[i] = cdiv(out[i], tr);
+  __syncwarp();
+}
+
+// A whole asynchronous sweep in one CTA, for graphs of small nodes: the
+// warps take the half-edges of a level (one each), a __syncthreads closes the
+// level, then the edge pass. No grid barrier; bit-identical to the per-level
+// launches. Per warp: out (max_chi^2) and two slices in shared memory.
+constexpr int ONECTA_THREADS = 1024;
+__host__ __device__ inline size_t onecta_warp_elems(int max_slice, int max_chi) {
+  return (size_t)max_chi * max_chi + 2 * (size_t)max_slice;
+}
+
+__global__ void __launch_bounds__(ONECTA_THREADS) bp_sweep_onecta_kernel(
+    dqz_graph_t g, const cd *__restrict__ T, const cd *n2e_old, const cd *e2n_old, cd *n2e_new, cd *e2n_new,
+    const uint8_t *__restrict__ src_sel, const uint8_t *__restrict__ edge_new, const int32_t *__restrict__ halves,
+    const int32_t *__restrict__ level_off, int n_levels, int max_slice, int max_chi) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  cd *out = reinterpret_cast<cd *>(smem_raw) + (size_t)warp * onecta_warp_elems(max_slice, max_chi);
+  cd *bufA = out + (size_t)max_chi * max_chi;
+  cd *bufB = bufA + max_slice;
+  for (int lv = 0; lv < n_levels; ++lv) {
+    for (int item = level_off[lv] + warp; item < level_off[lv + 1]; item += nw)
+      warp_node_update_half(g, T, n2e_old, e2n_old, n2e_new, src_sel, halves[item], out, bufA, bufB);
+    __syncthreads();
+  }
+  for (int h = warp; h < g.n_halves; h += nw) {
+    const int e = g.half_edge[h];
+    const int tw = g.half_twin[h];
+    if (e < 0 || tw < 0) continue;
+    const int c = g.edge_chi[e];
+    const cd *src = (edge_new[h] ? n2e_new : n2e_old) + g.half_msg_off[tw];
+    cd *dst = e2n_new + g.half_msg_off[h];
+    warp_copy16(reinterpret_cast<uint4 *>(dst), reinterpret_cast<const uint4 *>(src), c * c);
+  }
+}
+
 // Grid-wide barrier for a cooperative launch: one arrival counter and one
 // generation word (sync[0], sync[1], zero at launch). The last block to arrive
 // resets the counter and advances the generation; the others poll it, at
@@ -412,6 +520,25 @@ extern "C" int dqz_bp_sweep_levels(const dqz_graph_t *g, const void *tensors, co
       !level_off || !sync || !error_flag || n_levels <= 0 || max_level <= 0 || max_slice <= 0)
     return DQZ_ERR_ARG;
   if (max_chi <= 0 || max_chi > DQZ_MAX_CHI) return DQZ_ERR_UNSUPPORTED;
+  // Small nodes (bond slices up to 256 elements) and narrow levels (at most
+  // two half-edges per warp): the whole sweep in one CTA, a warp per
+  // half-edge and __syncthreads between levels (no grid barrier). Knob
+  // DQZ_TUNE_SWEEP_ONECTA: 1 = never, 2 = wherever the warps' buffers fit.
+  {
+    const int knob = dqz_get_tuning(DQZ_TUNE_SWEEP_ONECTA);
+    const size_t per_warp = onecta_warp_elems(max_slice, max_chi) * sizeof(cd);
+    int warps = (int)(BP_SMEM_LIMIT / per_warp);
+    if (warps > ONECTA_THREADS / 32) warps = ONECTA_THREADS / 32;
+    const bool rule = max_slice <= 256 && warps >= 8 && max_level <= 2 * warps;
+    if (knob != 1 && warps >= 1 && (rule || knob == 2)) {
+      DQZ_SMEM_ATTR_ONCE(bp_sweep_onecta_kernel, BP_SMEM_LIMIT);
+      bp_sweep_onecta_kernel<<<1, 32 * warps, (size_t)warps * per_warp, stream>>>(
+          *g, (const cd *)tensors, (const cd *)n2e_old, (const cd *)e2n_old, (cd *)n2e_new, (cd *)e2n_new, src_sel,
+          edge_new, halves, level_off, (int)n_levels, (int)max_slice, (int)max_chi);
+      DQZ_CHECK_LAUNCH();
+      return DQZ_OK;
+    }
+  }
   const size_t smem = bp_smem_bytes(max_slice, max_chi, false);
   if (smem > BP_SMEM_LIMIT) return DQZ_ERR_UNSUPPORTED;  // the per-level launches use global scratch then
   DQZ_SMEM_ATTR_ONCE(bp_sweep_levels_kernel, BP_SMEM_LIMIT);

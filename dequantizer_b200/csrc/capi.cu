@@ -10,7 +10,7 @@ extern "C" int dqz_device_supported(int device) {
 }
 
 namespace {
-int32_t g_tuning[DQZ_TUNE_COUNT] = {0, 0, 0, 0, 0};
+int32_t g_tuning[DQZ_TUNE_COUNT] = {0, 0, 0, 0, 0, 0};
 }
 
 extern "C" int dqz_set_tuning(int32_t knob, int32_t value) {
@@ -18,6 +18,7 @@ extern "C" int dqz_set_tuning(int32_t knob, int32_t value) {
   if ((knob == DQZ_TUNE_GAUGE_EDGE_WARPS || knob == DQZ_TUNE_GAUGE_DIST_WARPS) && value > 8) return DQZ_ERR_ARG;
   if (knob == DQZ_TUNE_GAUGE_PATH && value > 2) return DQZ_ERR_ARG;
   if (knob == DQZ_TUNE_SU_ONCHIP && value > 3) return DQZ_ERR_ARG;
+  if (knob == DQZ_TUNE_SWEEP_ONECTA && value > 2) return DQZ_ERR_ARG;
   g_tuning[knob] = value;
   return DQZ_OK;
 }

@@ -81,7 +81,9 @@ int dqz_device_supported(int device); /* 1 when the device is sm_100 */
 #define DQZ_TUNE_SU_ONCHIP 4        /* simple update: 1 = one-CTA global-scratch kernel only,
                                        2 = cluster forms at any batch size, 3 = no global-workspace
                                        cluster form                                               */
-#define DQZ_TUNE_COUNT 5
+#define DQZ_TUNE_SWEEP_ONECTA 5     /* asynchronous one-launch sweep in one CTA: 1 = never,
+                                       2 = wherever its warps' buffers fit                     */
+#define DQZ_TUNE_COUNT 6
 int dqz_set_tuning(int32_t knob, int32_t value); /* DQZ_ERR_ARG for an unknown knob or value < 0 */
 int32_t dqz_get_tuning(int32_t knob);            /* -1 for an unknown knob */
 
@@ -156,7 +158,10 @@ int dqz_pack_bf16_umma_nodes(const dqz_graph_t *g, const void *tensors_c64, void
  * dqz_bp_edge_pass, bit for bit. sync: two device words of scratch (zeroed by
  * the call). A barrier wait that runs out (seconds) sets *error_flag to 3 and
  * ends the launch. DQZ_ERR_UNSUPPORTED when a slice does not fit in shared
- * memory (use the per-level launches then). */
+ * memory (use the per-level launches then). Small nodes (slices up to 256
+ * elements) with narrow levels run in one CTA instead: a warp per half-edge,
+ * a CTA barrier between levels, the same results (knob
+ * DQZ_TUNE_SWEEP_ONECTA). */
 int dqz_bp_sweep_levels(const dqz_graph_t *g, const void *tensors, const void *n2e_old, const void *e2n_old,
                         void *n2e_new, void *e2n_new, const uint8_t *src_sel, const uint8_t *edge_new,
                         const int32_t *halves, const int32_t *level_off, int32_t n_levels, int32_t max_level,

@@ -18,10 +18,12 @@ def _reset_knobs():
 
 def test_knobs_roundtrip_and_validation():
     lib = _lib.lib()
-    cfg = {"gauge_edge_warps": 4, "gauge_dist_warps": 2, "gauge_path": 1, "su_grid": 100, "su_onchip": 1}
+    cfg = {"gauge_edge_warps": 4, "gauge_dist_warps": 2, "gauge_path": 1, "su_grid": 100, "su_onchip": 1,
+           "sweep_onecta": 2}
     autotune.set_knobs(cfg)
     assert autotune.get_knobs() == cfg
     assert lib.dqz_set_tuning(autotune.KNOBS["su_onchip"], 4) == _lib.DQZ_ERR_ARG
+    assert lib.dqz_set_tuning(autotune.KNOBS["sweep_onecta"], 3) == _lib.DQZ_ERR_ARG
     assert lib.dqz_set_tuning(autotune.KNOBS["gauge_edge_warps"], 9) == _lib.DQZ_ERR_ARG
     assert lib.dqz_set_tuning(autotune.KNOBS["gauge_path"], 3) == _lib.DQZ_ERR_ARG
     assert lib.dqz_set_tuning(99, 1) == _lib.DQZ_ERR_ARG

@@ -424,14 +424,28 @@ def test_gauge_knobs_leave_results_unchanged_and_tuner_caches(tmp_path):
         autotune.set_knobs({k: 0 for k in autotune.KNOBS})
 
 
-@pytest.mark.parametrize("case", ["lattice_3x3x3", "eagle_cell_4", "eagle_cell_8_16", "eagle_cell_32"])
-def test_one_launch_sweep_equals_level_launches(case):
+@pytest.mark.parametrize("case,onecta", [("lattice_3x3x3", 0), ("lattice_3x3x3", 1), ("eagle_cell_4", 0),
+                                         ("eagle_cell_4", 1), ("eagle_cell_8_16", 0), ("eagle_cell_32", 0)])
+def test_one_launch_sweep_equals_level_launches(case, onecta):
     """The one-launch asynchronous sweep (every node level of the DFS schedule
-    and the edge pass in one cooperative launch, grid barriers between levels:
-    dqz_bp_sweep_levels below bond 8, dqz_bp_sweep_sliced with one work item
-    per bond slice from bond 8) gives one dqz_bp_node_update launch per level
-    plus dqz_bp_edge_pass, bit for bit, over several sweeps; mixed bonds of 8
-    and 16 give levels of uneven item counts."""
+    and the edge pass in one launch: below bond 8 one CTA with a warp per
+    half-edge and CTA barriers between levels (small nodes, the default) or a
+    cooperative grid with grid barriers (dqz_bp_sweep_levels, knob
+    sweep_onecta = 1); from bond 8 dqz_bp_sweep_sliced with one work item per
+    bond slice) gives one dqz_bp_node_update launch per level plus
+    dqz_bp_edge_pass, bit for bit, over several sweeps; mixed bonds of 8 and
+    16 give levels of uneven item counts."""
+    from dequantizer_b200 import _lib, autotune
+    from dequantizer_b200.layout import GraphLayout
+
+    autotune.set_knobs({"sweep_onecta": onecta})
+    try:
+        _one_launch_sweep_case(case)
+    finally:
+        autotune.set_knobs({"sweep_onecta": 0})
+
+
+def _one_launch_sweep_case(case):
     from dequantizer_b200 import _lib
     from dequantizer_b200.layout import GraphLayout
 
