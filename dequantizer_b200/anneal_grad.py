@@ -326,6 +326,13 @@ class AnnealingGradient:
                             "oa": others(1, 2), "ob": others(3, 4)})
             levels.append(out)
         t["levels"] = levels
+        # each level's groups concatenated, in group order
+        t["level_cat"] = [{"gates": [j for grp in out for j in grp["gates"]],
+                           "sizes": [len(grp["gates"]) for grp in out],
+                           "e": torch.cat([grp["e"] for grp in out]),
+                           "ab": torch.cat([grp["a"] for grp in out] + [grp["b"] for grp in out]),
+                           "oa": torch.cat([grp["oa"] for grp in out]),
+                           "ob": torch.cat([grp["ob"] for grp in out])} for out in levels]
         for e in self.edges:
             e.dimension = c
         t["problem"] = FixedPointProblem(self.graph, topo=self.topo)
@@ -343,25 +350,25 @@ class AnnealingGradient:
 
     def _coupling_layer_stacked(self, G, L, tau):
         """coupling_layer on the stacked form: per level, the gates grouped by
-        their bond slots, one batch each, written back with one index_copy."""
+        their bond slots only to bring the gate bond first (one gather and
+        movedim per group), then one batch for the whole level (one QR / SVD
+        call: the solver calls have a fixed cost each), written back with one
+        index_copy per level."""
         t = self._stacked_tables()
         k = self.uniform_degree
-        for groups in t["levels"]:
-            idx, new, eidx, lnew = [], [], [], []
-            for grp in groups:
-                h1, h2 = self.coupling_halves(tau, grp["gates"])
-                ia, ib = grp["ia"], grp["ib"]
-                Xa = torch.movedim(G[grp["a"]], 1 + ia, 1)
-                Xb = torch.movedim(G[grp["b"]], 1 + ib, 1)
-                oa = [L[grp["oa"][:, p]] for p in range(k - 1)]
-                ob = [L[grp["ob"][:, p]] for p in range(k - 1)]
-                qa, qb, lk = self._su_core(Xa, oa, Xb, ob, L[grp["e"]], h1, h2)
-                idx += [grp["a"], grp["b"]]
-                new += [torch.movedim(qa, qa.dim() - 1, 1 + ia), torch.movedim(qb, qb.dim() - 1, 1 + ib)]
-                eidx.append(grp["e"])
-                lnew.append(lk)
-            G = G.index_copy(0, torch.cat(idx), torch.cat(new))
-            L = L.index_copy(0, torch.cat(eidx), torch.cat(lnew))
+        for groups, cat in zip(t["levels"], t["level_cat"]):
+            Xa = torch.cat([torch.movedim(G[grp["a"]], 1 + grp["ia"], 1) for grp in groups])
+            Xb = torch.cat([torch.movedim(G[grp["b"]], 1 + grp["ib"], 1) for grp in groups])
+            oa = [L[cat["oa"][:, p]] for p in range(k - 1)]
+            ob = [L[cat["ob"][:, p]] for p in range(k - 1)]
+            h1, h2 = self.coupling_halves(tau, cat["gates"])
+            qa, qb, lk = self._su_core(Xa, oa, Xb, ob, L[cat["e"]], h1, h2)
+            new_a, new_b = [], []
+            for grp, xa, xb in zip(groups, qa.split(cat["sizes"]), qb.split(cat["sizes"])):
+                new_a.append(torch.movedim(xa, xa.dim() - 1, 1 + grp["ia"]))
+                new_b.append(torch.movedim(xb, xb.dim() - 1, 1 + grp["ib"]))
+            G = G.index_copy(0, cat["ab"], torch.cat(new_a + new_b))
+            L = L.index_copy(0, cat["e"], lk)
         return G, L
 
     def _regauge_stacked(self, G, L):
