@@ -321,7 +321,11 @@ __global__ void __launch_bounds__(BP_THREADS) bp_sweep_levels_kernel(
 // the outgoing message; after a grid barrier each half-edge of the level is
 // divided by its trace; a second barrier closes the level. Same arithmetic and
 // order as bp_node_generic, so the messages are bit-identical.
-__global__ void __launch_bounds__(BP_THREADS) bp_sweep_sliced_kernel(
+// Twice the threads of the per-level kernels: a level's items all run at
+// once, so the level lasts as long as one item, and more threads per item
+// shorten it (two CTAs of 512 threads still fit per SM).
+constexpr int SLICED_THREADS = 512;
+__global__ void __launch_bounds__(SLICED_THREADS) bp_sweep_sliced_kernel(
     dqz_graph_t g, const cd *__restrict__ T, const cd *n2e_old, const cd *e2n_old, cd *n2e_new, cd *e2n_new,
     const uint8_t *__restrict__ src_sel, const uint8_t *__restrict__ edge_new, const int32_t *__restrict__ halves,
     const int32_t *__restrict__ level_off, const int32_t *__restrict__ item_half,
@@ -599,7 +603,7 @@ extern "C" int dqz_bp_sweep_sliced(const dqz_graph_t *g, const void *tensors, co
   int dev = 0, sms = 148, per_sm = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return DQZ_ERR_CUDA;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bp_sweep_sliced_kernel, BP_THREADS, smem) !=
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bp_sweep_sliced_kernel, SLICED_THREADS, smem) !=
           cudaSuccess ||
       per_sm < 1)
     return DQZ_ERR_UNSUPPORTED;
@@ -608,7 +612,7 @@ extern "C" int dqz_bp_sweep_sliced(const dqz_graph_t *g, const void *tensors, co
   if (cudaMemsetAsync(sync, 0, 2 * sizeof(uint32_t), stream) != cudaSuccess) return DQZ_ERR_CUDA;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(grid);
-  cfg.blockDim = dim3(BP_THREADS);
+  cfg.blockDim = dim3(SLICED_THREADS);
   cfg.dynamicSmemBytes = smem;
   cfg.stream = stream;
   cudaLaunchAttribute attr[1];
