@@ -163,41 +163,57 @@ __device__ __forceinline__ void warp_mode_product(const cd *__restrict__ X, cd *
 __device__ __forceinline__ void warp_node_update_half(const dqz_graph_t &g, const cd *__restrict__ T, const cd *n2e_old,
                                                       const cd *e2n_old, cd *n2e_new,
                                                       const uint8_t *__restrict__ src_sel, int h, cd *out, cd *bufA,
-                                                      cd *bufB) {
+                                                      cd *bufB, cd *Ts, cd *Ms) {
   const int lane = threadIdx.x & 31;
   const int v = g.half_node[h];
   NodeShape s;
   load_shape(g, v, s);
   const int e = h - s.half0;
   const int ce = s.dims[e];
-  const cd *Tv = T + g.node_off[v];
   const unsigned Re = (unsigned)s.stride[e];
   const unsigned P = (unsigned)(s.size / ce);
   const FastDiv fRe(Re);
+  // the node tensor and the k-1 incoming messages staged once (their global
+  // loads all in flight together), then everything runs from shared memory
+  {
+    const cd *Tv = T + g.node_off[v];
+    for (unsigned x = lane; x < (unsigned)s.size; x += 32) Ts[x] = Tv[x];
+    int off = 0;
+    for (int f = 0; f < s.k; ++f) {
+      if (f == e) continue;
+      const int q2 = s.dims[f] * s.dims[f];
+      const cd *m = incoming_msg(g, s.half0 + f, n2e_old, e2n_old, n2e_new, src_sel);
+      for (int x = lane; x < q2; x += 32) Ms[off + x] = m[x];
+      off += q2;
+    }
+    __syncwarp();
+  }
   for (int a = 0; a < ce; ++a) {
     for (unsigned x = lane; x < P; x += 32) {
       const unsigned l = fRe.div(x), r = x - l * Re;
-      bufA[x] = Tv[(l * (unsigned)ce + (unsigned)a) * Re + r];
+      bufA[x] = Ts[(l * (unsigned)ce + (unsigned)a) * Re + r];
     }
     __syncwarp();
     cd *cur = bufA, *nxt = bufB;
     unsigned Lj = 1;
+    int off = 0;
     for (int f = 0; f < s.k; ++f) {
       if (f == e) continue;
       const int q = s.dims[f];
       const unsigned R = P / Lj / (unsigned)q;
-      warp_mode_product(cur, nxt, Lj, q, R, incoming_msg(g, s.half0 + f, n2e_old, e2n_old, n2e_new, src_sel));
+      warp_mode_product(cur, nxt, Lj, q, R, Ms + off);
       __syncwarp();
       cd *t = cur;
       cur = nxt;
       nxt = t;
       Lj *= (unsigned)q;
+      off += q * q;
     }
     for (int ap = 0; ap < ce; ++ap) {
       cd acc = czero();
       for (unsigned x = lane; x < P; x += 32) {
         const unsigned l = fRe.div(x), r = x - l * Re;
-        cfmac(acc, Tv[(l * (unsigned)ce + (unsigned)ap) * Re + r], cur[x]);
+        cfmac(acc, Ts[(l * (unsigned)ce + (unsigned)ap) * Re + r], cur[x]);
       }
       acc = warp_csum(acc);
       if (lane == 0) out[ap * ce + a] = acc;
@@ -219,8 +235,11 @@ __device__ __forceinline__ void warp_node_update_half(const dqz_graph_t &g, cons
 // level, then the edge pass. No grid barrier; bit-identical to the per-level
 // launches. Per warp: out (max_chi^2) and two slices in shared memory.
 constexpr int ONECTA_THREADS = 1024;
+// per warp: out (max_chi^2), two slices, the node tensor (max_slice x max_chi),
+// the incoming messages ((DQZ_MAX_DEGREE - 1) x max_chi^2)
 __host__ __device__ inline size_t onecta_warp_elems(int max_slice, int max_chi) {
-  return (size_t)max_chi * max_chi + 2 * (size_t)max_slice;
+  return (size_t)max_chi * max_chi + 2 * (size_t)max_slice + (size_t)max_slice * max_chi +
+         (size_t)(DQZ_MAX_DEGREE - 1) * max_chi * max_chi;
 }
 
 __global__ void __launch_bounds__(ONECTA_THREADS) bp_sweep_onecta_kernel(
@@ -232,9 +251,11 @@ __global__ void __launch_bounds__(ONECTA_THREADS) bp_sweep_onecta_kernel(
   cd *out = reinterpret_cast<cd *>(smem_raw) + (size_t)warp * onecta_warp_elems(max_slice, max_chi);
   cd *bufA = out + (size_t)max_chi * max_chi;
   cd *bufB = bufA + max_slice;
+  cd *Ts = bufB + max_slice;
+  cd *Ms = Ts + (size_t)max_slice * max_chi;
   for (int lv = 0; lv < n_levels; ++lv) {
     for (int item = level_off[lv] + warp; item < level_off[lv + 1]; item += nw)
-      warp_node_update_half(g, T, n2e_old, e2n_old, n2e_new, src_sel, halves[item], out, bufA, bufB);
+      warp_node_update_half(g, T, n2e_old, e2n_old, n2e_new, src_sel, halves[item], out, bufA, bufB, Ts, Ms);
     __syncthreads();
   }
   for (int h = warp; h < g.n_halves; h += nw) {
