@@ -123,11 +123,19 @@ __device__ __forceinline__ void load_shape(const dqz_graph_t &g, int v, NodeShap
 // m = floor(2^32 (2^s - d) / d) + 1 (< 2^32), x / d = (umulhi(x, m) + x) >> s
 // for every 32-bit x. A hardware-free integer division costs a long
 // instruction sequence; this one a multiply-high, an add and a shift.
+// For d < 2^21 the multiplier comes from one correctly rounded double
+// division: the numerator 2^32 (2^s - d) is exact in a double, and the exact
+// quotient is never within the division's rounding error of an integer
+// (checked exhaustively for every such d), so its floor is exact.
 struct FastDiv {
   unsigned d, m, s;
   __device__ __forceinline__ explicit FastDiv(unsigned dv) : d(dv) {
     s = dv > 1 ? 32u - (unsigned)__clz(dv - 1u) : 0u;
-    m = (unsigned)((((1ull << 32) * ((1ull << s) - dv)) / dv) + 1ull);
+    const unsigned long long num = (1ull << 32) * ((1ull << s) - dv);
+    if (dv < (1u << 21))
+      m = (unsigned)((unsigned long long)floor((double)num / (double)dv) + 1ull);
+    else
+      m = (unsigned)(num / dv + 1ull);
   }
   __device__ __forceinline__ unsigned div(unsigned x) const {
     return (unsigned)(((unsigned long long)__umulhi(x, m) + x) >> s);
