@@ -136,16 +136,20 @@ __device__ void su_load_side(const dqz_graph_t &g, const double *lambdas, int h,
 // Decompose row R = (other bonds in order, o): returns the tensor offset
 // without the slot bond and the physical index, and the product of
 // lambda weights (or of their safe inverses).
-__device__ __forceinline__ long long su_row(const SUSide &S, long long R, int &o, double &wt, bool inverse,
+// (32-bit index arithmetic: the entry points refuse rows x columns >= 2^31)
+__device__ __forceinline__ long long su_row(const SUSide &S, unsigned R, int &o, double &wt, bool inverse,
                                             double eps) {
-  o = (int)(R % S.d);
-  long long rem = R / S.d;
+  const unsigned rd = R / (unsigned)S.d;
+  o = (int)(R - rd * (unsigned)S.d);
+  unsigned rem = rd;
   long long off = 0;
   wt = 1.0;
   for (int f = S.k - 1; f >= 0; --f) {
     if (f == S.slot) continue;
-    const int a = (int)(rem % S.dims[f]);
-    rem /= S.dims[f];
+    const unsigned df = (unsigned)S.dims[f];
+    const unsigned rq = rem / df;
+    const int a = (int)(rem - rq * df);
+    rem = rq;
     off += a * S.stride[f];
     const double l = S.lam[f][a];
     wt *= inverse ? safe_inverse(l, eps) : l;
@@ -157,12 +161,12 @@ __device__ __forceinline__ long long su_row(const SUSide &S, long long R, int &o
 __device__ void su_build(const SUSide &S, const cd *T, const cd *H, int r, cd *A, double *red) {
   const int ce = S.dims[S.slot];
   const int K = ce * r;
-  const long long MK = (long long)S.M * K;
+  const unsigned MK = (unsigned)S.M * (unsigned)K;
   const int d = S.d;
   double n2 = 0.0;
-  for (long long idx = threadIdx.x; idx < MK; idx += blockDim.x) {
-    const long long R = idx % S.M;
-    const int C = (int)(idx / S.M);
+  for (unsigned idx = threadIdx.x; idx < MK; idx += blockDim.x) {
+    const unsigned C = idx / (unsigned)S.M;
+    const unsigned R = idx - C * (unsigned)S.M;
     const int ae = C / r, rho = C % r;
     int o;
     double wt;
@@ -175,7 +179,7 @@ __device__ void su_build(const SUSide &S, const cd *T, const cd *H, int r, cd *A
   }
   n2 = block_sum(n2, red);
   const double inv = 1.0 / sqrt(n2);
-  for (long long idx = threadIdx.x; idx < MK; idx += blockDim.x) A[idx] = cscale(A[idx], inv);
+  for (unsigned idx = threadIdx.x; idx < MK; idx += blockDim.x) A[idx] = cscale(A[idx], inv);
   __syncthreads();
 }
 
@@ -188,18 +192,21 @@ __device__ void su_write(const SUSide &S, const cd *X, int rank, cd *T, double e
     nst[f] = st;
     st *= (f == S.slot) ? rank : S.dims[f];
   }
-  const long long total = (long long)S.M * rank;
-  for (long long idx = threadIdx.x; idx < total; idx += blockDim.x) {
-    const long long R = idx % S.M;
-    const int c = (int)(idx / S.M);
-    const int o = (int)(R % S.d);
-    long long rem = R / S.d;
+  const unsigned total = (unsigned)S.M * (unsigned)rank;
+  for (unsigned idx = threadIdx.x; idx < total; idx += blockDim.x) {
+    const unsigned c = idx / (unsigned)S.M;
+    const unsigned R = idx - c * (unsigned)S.M;
+    const unsigned rd = R / (unsigned)S.d;
+    const int o = (int)(R - rd * (unsigned)S.d);
+    unsigned rem = rd;
     long long off = o + (long long)c * nst[S.slot];
     double wt = 1.0;
     for (int f = S.k - 1; f >= 0; --f) {
       if (f == S.slot) continue;
-      const int a = (int)(rem % S.dims[f]);
-      rem /= S.dims[f];
+      const unsigned df = (unsigned)S.dims[f];
+      const unsigned rq = rem / df;
+      const int a = (int)(rem - rq * df);
+      rem = rq;
       off += a * nst[f];
       wt *= safe_inverse(S.lam[f][a], eps);
     }
@@ -480,18 +487,21 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(SUF_THREADS, 1)
     // ---- B[b, (a, i)] = wt(b) T[.., a, .., i], column-major (ld MB)
     {
       const int ce = X.dims[X.slot];
-      const long long total = (long long)D.MB * D.KB;
-      for (long long idx = tid; idx < total; idx += nt) {
-        const int i = (int)(idx % d);
-        const long long t = idx / d;
-        const int a = (int)(t % ce);
-        const int b = (int)(t / ce);
-        long long rem = b, off = 0;
+      const int total = D.MB * D.KB;
+      for (int idx = tid; idx < total; idx += nt) {
+        const int i = idx % d;
+        const int t = idx / d;
+        const int a = t % ce;
+        const int b = t / ce;
+        unsigned rem = (unsigned)b;
+        long long off = 0;
         double wt = 1.0;
         for (int f = X.k - 1; f >= 0; --f) {
           if (f == X.slot) continue;
-          const int af = (int)(rem % X.dims[f]);
-          rem /= X.dims[f];
+          const unsigned df = (unsigned)X.dims[f];
+          const unsigned rq = rem / df;
+          const int af = (int)(rem - rq * df);
+          rem = rq;
           off += af * X.stride[f];
           wt *= X.lam[f][af];
         }
@@ -644,13 +654,15 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(SUF_THREADS, 1)
       }
     }
     __syncthreads();
-    // V^H Z (k x p): Z[row, q = col * d + o] = X[row * d + o, col] for row < k
-    for (int idx = tid; idx < k * p; idx += nt) {
-      const int c = idx % k, q = idx / k;
+    // V^H Z (k x p): Z[row, q = col * d + o] = X[row * d + o, col] for row < k;
+    // one warp per entry, lanes over rows (column c of V is contiguous)
+    for (int pr = warp; pr < k * p; pr += nw) {
+      const int c = pr % k, q = pr / k;
       const int col = q / d, o = q % d;
       cd v = czero();
-      for (int row = c; row < k; ++row) cfmac(v, vb(row, c), Xm[(row * d + o) + (long long)col * D.MS]);
-      G[idx] = v;
+      for (int row = c + lane; row < k; row += 32) cfmac(v, vb(row, c), Xm[(row * d + o) + (long long)col * D.MS]);
+      v = warp_csum(v);
+      if (lane == 0) G[pr] = v;
     }
     __syncthreads();
     for (int q = tid; q < p; q += nt) {  // in place: G[:, q] <- T G[:, q] (row i reads rows >= i)
@@ -670,21 +682,27 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(SUF_THREADS, 1)
         nst[f] = st;
         st *= (f == X.slot) ? rank : X.dims[f];
       }
-      const long long total = (long long)D.MB * p;
-      for (long long idx = tid; idx < total; idx += nt) {
-        const int q = (int)(idx % p);
-        const int b = (int)(idx / p);
+      // consecutive threads take consecutive rows b: V's columns are read
+      // contiguously and G[:, q] is one broadcast (q-major threads had every
+      // lane of a warp on its own row of G, one shared-memory bank)
+      const int total = D.MB * p;
+      for (int idx = tid; idx < total; idx += nt) {
+        const int b = idx % D.MB;
+        const int q = idx / D.MB;
         const int col = q / d, o = q % d;
         cd v = b < k ? Xm[(b * d + o) + (long long)col * D.MS] : czero();
         const cd *gq = G + (long long)q * k;
         const int cmax = b < k ? b : k - 1;
         for (int c = 0; c <= cmax; ++c) v = csub(v, cmul(vb(b, c), gq[c]));
-        long long rem = b, off = o + (long long)col * nst[X.slot];
+        unsigned rem = (unsigned)b;
+        long long off = o + (long long)col * nst[X.slot];
         double wt = 1.0;
         for (int f = X.k - 1; f >= 0; --f) {
           if (f == X.slot) continue;
-          const int af = (int)(rem % X.dims[f]);
-          rem /= X.dims[f];
+          const unsigned df = (unsigned)X.dims[f];
+          const unsigned rq = rem / df;
+          const int af = (int)(rem - rq * df);
+          rem = rq;
           off += af * nst[f];
           wt *= safe_inverse(X.lam[f][af], eps);
         }
@@ -756,7 +774,7 @@ extern "C" int dqz_simple_update(const dqz_graph_t *g, void *tensors, double *la
   if (!g || !tensors || !lambdas || !edges || !ctrl_is_first || !halves || !ranks || !err || !entropy || !scratch)
     return DQZ_ERR_ARG;
   if (n < 0 || max_rows <= 0 || max_cols <= 0) return DQZ_ERR_ARG;
-  if (max_cols > DQZ_MAX_CHI) return DQZ_ERR_UNSUPPORTED;
+  if (max_cols > DQZ_MAX_CHI || (long long)max_rows * max_cols >= (1ll << 31)) return DQZ_ERR_UNSUPPORTED;
   if (n == 0) return DQZ_OK;
   const size_t smem = su_smem_bytes(max_cols);
   if (smem > SMEM_LIMIT) return DQZ_ERR_UNSUPPORTED;
@@ -847,7 +865,7 @@ extern "C" int dqz_simple_update_noalloc(const dqz_graph_t *g, void *tensors, do
   if (!g || !tensors || !lambdas || !edges || !ctrl_is_first || !halves || !ranks || !err || !entropy)
     return DQZ_ERR_ARG;
   if (n < 0 || max_rows <= 0 || max_cols <= 0) return DQZ_ERR_ARG;
-  if (max_cols > DQZ_MAX_CHI) return DQZ_ERR_UNSUPPORTED;
+  if (max_cols > DQZ_MAX_CHI || (long long)max_rows * max_cols >= (1ll << 31)) return DQZ_ERR_UNSUPPORTED;
   const size_t per_job = su_scratch_per_job(max_rows, max_cols);
   if (per_job > (size_t)DQZ_NOALLOC_SCRATCH_BYTES) return DQZ_ERR_UNSUPPORTED;
   if (n == 0) return DQZ_OK;
