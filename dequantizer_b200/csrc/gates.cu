@@ -654,26 +654,41 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(SUF_THREADS, 1)
       }
     }
     __syncthreads();
-    // V^H Z (k x p): Z[row, q = col * d + o] = X[row * d + o, col] for row < k;
-    // one warp per entry, lanes over rows (column c of V is contiguous)
-    for (int pr = warp; pr < k * p; pr += nw) {
-      const int c = pr % k, q = pr / k;
+    // V^H Z (k x p): Z[row, q = col * d + o] = X[row * d + o, col] for row < k
+    for (int idx = tid; idx < k * p; idx += nt) {
+      const int c = idx % k, q = idx / k;
       const int col = q / d, o = q % d;
       cd v = czero();
-      for (int row = c + lane; row < k; row += 32) cfmac(v, vb(row, c), Xm[(row * d + o) + (long long)col * D.MS]);
-      v = warp_csum(v);
-      if (lane == 0) G[pr] = v;
+      for (int row = c; row < k; ++row) cfmac(v, vb(row, c), Xm[(row * d + o) + (long long)col * D.MS]);
+      G[idx] = v;
     }
     __syncthreads();
-    for (int q = tid; q < p; q += nt) {  // in place: G[:, q] <- T G[:, q] (row i reads rows >= i)
-      cd *gq = G + (long long)q * k;
-      for (int i = 0; i < k; ++i) {
-        cd v = czero();
-        for (int l = i; l < k; ++l) cfma(v, Tw[i + (long long)l * k], gq[l]);
-        gq[i] = v;
+    // G <- T G: one thread per entry (rows i consecutive: T's column reads
+    // contiguous, G's a broadcast), held in registers across a barrier and
+    // written in place, a chunk of entries at a time in increasing index: an
+    // entry reads rows >= its own of its column, which earlier chunks never write
+    for (int base = 0; base < k * p; base += 8 * nt) {
+      cd vals[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const int idx = base + tid + u * nt;
+        vals[u] = czero();
+        if (idx < k * p) {
+          const int i = idx % k, q = idx / k;
+          const cd *gq = G + (long long)q * k;
+          cd v = czero();
+          for (int l = i; l < k; ++l) cfma(v, Tw[i + (long long)l * k], gq[l]);
+          vals[u] = v;
+        }
       }
+      __syncthreads();
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const int idx = base + tid + u * nt;
+        if (idx < k * p) G[idx] = vals[u];
+      }
+      __syncthreads();
     }
-    __syncthreads();
     // ---- Gamma[b, .., col, .., o] = ((Q_B Z)[b, q]) * prod safe_inv(lambda), bond `rank`
     {
       long long nst[DQZ_MAX_DEGREE];
