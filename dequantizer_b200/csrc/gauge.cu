@@ -76,15 +76,8 @@ __global__ void __launch_bounds__(GAUGE_THREADS) vidal_edges_kernel(dqz_graph_t 
       Ab[i] = mb[i];
     }
     __syncthreads();
-    // the two eigendecompositions at once, one warp each (bonds up to 64: at
-    // most 32 pairs a rotation step), no CTA barrier per step
-    {
-      __shared__ Rot rots_b[DQZ_MAX_CHI / 2 + 1];
-      const int warp = tid >> 5;
-      if (warp == 0) warp_herm_eigh(Af, c, Vf, c, c, wf, rots);
-      if (warp == 1) warp_herm_eigh(Ab, c, Vb, c, c, wb, rots_b);
-      __syncthreads();
-    }
+    herm_eigh(Af, c, Vf, c, c, wf, rots, red);
+    herm_eigh(Ab, c, Vb, c, c, wb, rots, red);
     sqrt_weights(wf, wif, c, eps, tid, nt);
     sqrt_weights(wb, wib, c, eps, tid, nt);
     __syncthreads();
@@ -114,8 +107,7 @@ __global__ void __launch_bounds__(GAUGE_THREADS) vidal_edges_kernel(dqz_graph_t 
       C[j * c + i] = acc;
     }
     __syncthreads();
-    if ((tid >> 5) == 0) warp_hestenes(C, c, c, c, W, c, sv);
-    __syncthreads();
+    hestenes(C, c, c, c, W, c, sv, flag, red);
     sort_desc(sv, c, perm);
     // lambda = sigma / |sigma|, truncated; U (into Af) and V^* (into Ab)
     // masked and Frobenius-normalised.

@@ -424,8 +424,6 @@ static __device__ void apply_q(const cd *A, int M, int kk, const cd *tau, cd *X,
 // singular vectors (null columns completed), s unsorted. V must have room for
 // zr x kk entries; X (kk x kk) and tau (kk) are scratch; acc (kk ints) is
 // overwritten. All in shared memory.
-static __device__ void warp_hestenes(cd *A, int lda, int m, int n, cd *V, int ldv, double *s, int max_sweeps = 60);
-
 static __device__ void hestenes_qr(cd *Z, int zr, int kk, cd *V, cd *X, cd *tau, double *s, int *flag, int *acc,
                                    double *red) {
   const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5;
@@ -435,14 +433,7 @@ static __device__ void hestenes_qr(cd *Z, int zr, int kk, cd *V, cd *X, cd *tau,
     X[idx] = j <= i ? cconj(Z[j + (long long)i * zr]) : czero();
   }
   __syncthreads();
-  // X = U_x S, V = V_x: one warp for kk <= 64 (a pair per lane, no CTA
-  // barrier per rotation round: the CTA form paid ~3k cycles a round at kk = 32)
-  if (kk <= 64) {
-    if (warp == 0) warp_hestenes(X, kk, kk, kk, V, kk, s, 60);
-    __syncthreads();
-  } else {
-    hestenes(X, kk, kk, kk, V, kk, s, flag, red);
-  }
+  hestenes(X, kk, kk, kk, V, kk, s, flag, red);  // X = U_x S, V = V_x
   // V_x (ld kk) spread to ld zr with zero rows kk..zr-1, last column first (new
   // positions lie at or after the old ones); one warp, kk <= 64 (two rows a lane)
   if (warp == 0 && zr != kk) {
@@ -561,9 +552,9 @@ static __device__ void warp_herm_eigh(cd *A, int lda, cd *V, int ldv, int n, dou
 }
 
 // One-sided Jacobi SVD (hestenes) of A (m x n, column-major, lda); lane i
-// rotates pair i of each round-robin step, looping over the rows itself
-// (n <= 64: at most 32 pairs a step). Same null-column rule as hestenes.
-static __device__ void warp_hestenes(cd *A, int lda, int m, int n, cd *V, int ldv, double *s, int max_sweeps) {
+// rotates pair i of each round-robin step, looping over the rows itself.
+// Same null-column rule as hestenes.
+static __device__ void warp_hestenes(cd *A, int lda, int m, int n, cd *V, int ldv, double *s, int max_sweeps = 60) {
   const int lane = threadIdx.x & 31;
   for (int i = lane; i < n * n; i += 32) V[(i / n) * ldv + (i % n)] = (i / n == i % n) ? mk(1.0, 0.0) : czero();
   const double tol = 1.1e-16 * sqrt((double)(m > 1 ? m : 1)) * 2.0;
