@@ -28,6 +28,8 @@ MAX_PHYS = 8
 SRC_E2N_OLD = 0
 SRC_N2E_OLD = 1
 SRC_N2E_NEW = 2
+PLAN_WORDS = 5 + MAX_DEGREE + MAX_DEGREE - 1  # DQZ_PLAN_WORDS
+TUNE_SWEEP_ONECTA = 5  # DQZ_TUNE_SWEEP_ONECTA
 
 
 class DqzError(RuntimeError):
@@ -80,6 +82,7 @@ _SIGNATURES = {
     "dqz_bp_node_scratch_bytes": (_S, [_I, _I, _I]),
     "dqz_bp_edge_pass": (ctypes.c_int, [_G, _P, _P, _P, _P, _I, _P]),
     "dqz_bp_sweep_levels": (ctypes.c_int, [_G, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I, _I, _I, _I, _P, _P, _P]),
+    "dqz_bp_sweep_planned": (ctypes.c_int, [_G, _P, _P, _P, _P, _P, _P, _P, _P, _I, _I, _I, _I, _P]),
     "dqz_bp_sweep_sliced": (ctypes.c_int, [_G, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I, _I, _I, _I, _P, _P,
                                            _P]),
     "dqz_bp_node_update_k3": (ctypes.c_int, [_G, _I, _I, _P, _P, _P, _P, _P, _P, _I, _P, _P]),

@@ -237,6 +237,7 @@ __device__ __forceinline__ void warp_node_update_half(const dqz_graph_t &g, cons
 constexpr int ONECTA_THREADS = 1024;
 // per warp: out (max_chi^2), two slices, the node tensor (max_slice x max_chi),
 // the incoming messages ((DQZ_MAX_DEGREE - 1) x max_chi^2)
+__host__ __device__ inline size_t round_up16(size_t x) { return (x + 15) & ~(size_t)15; }
 __host__ __device__ inline size_t onecta_warp_elems(int max_slice, int max_chi) {
   return (size_t)max_chi * max_chi + 2 * (size_t)max_slice + (size_t)max_slice * max_chi +
          (size_t)(DQZ_MAX_DEGREE - 1) * max_chi * max_chi;
@@ -256,6 +257,118 @@ __global__ void __launch_bounds__(ONECTA_THREADS) bp_sweep_onecta_kernel(
   for (int lv = 0; lv < n_levels; ++lv) {
     for (int item = level_off[lv] + warp; item < level_off[lv + 1]; item += nw)
       warp_node_update_half(g, T, n2e_old, e2n_old, n2e_new, src_sel, halves[item], out, bufA, bufB, Ts, Ms);
+    __syncthreads();
+  }
+  for (int h = warp; h < g.n_halves; h += nw) {
+    const int e = g.half_edge[h];
+    const int tw = g.half_twin[h];
+    if (e < 0 || tw < 0) continue;
+    const int c = g.edge_chi[e];
+    const cd *src = (edge_new[h] ? n2e_new : n2e_old) + g.half_msg_off[tw];
+    cd *dst = e2n_new + g.half_msg_off[h];
+    warp_copy16(reinterpret_cast<uint4 *>(dst), reinterpret_cast<const uint4 *>(src), c * c);
+  }
+}
+
+// ---- the one-CTA sweep with a host-built plan: per item (the order of the
+// level table) DQZ_PLAN_WORDS words: node offset, degree k, physical
+// dimension d, slot e of the outgoing bond, outgoing message offset, the k
+// bond dimensions (DQZ_MAX_DEGREE words), then per other bond in bond order
+// its incoming message as offset * 4 + source (DQZ_SRC_*). A warp reads its
+// item's words in one coalesced load instead of walking node -> half-edges
+// -> edges -> twins (six dependent loads), then stages the tensor and the
+// messages at once. Same arithmetic as warp_node_update_half.
+__device__ __forceinline__ void warp_plan_item(const long long *pw, const cd *__restrict__ T, const cd *n2e_old,
+                                               const cd *e2n_old, cd *n2e_new, cd *out, cd *bufA, cd *bufB, cd *Ts,
+                                               cd *Ms) {
+  const int lane = threadIdx.x & 31;
+  const int k = (int)pw[1], d = (int)pw[2], e = (int)pw[3];
+  const long long *dims = pw + 5;
+  unsigned size = (unsigned)d, Re = (unsigned)d;
+  for (int f = k - 1; f >= 0; --f) {
+    if (f == e) Re = size;
+    size *= (unsigned)dims[f];
+  }
+  const int ce = (int)dims[e];
+  const unsigned P = size / (unsigned)ce;
+  const FastDiv fRe(Re);
+  {
+    const cd *Tv = T + pw[0];
+    for (unsigned x = lane; x < size; x += 32) Ts[x] = Tv[x];
+    int off = 0, slot = 0;
+    for (int f = 0; f < k; ++f) {
+      if (f == e) continue;
+      const int q2 = (int)(dims[f] * dims[f]);
+      const long long code = pw[5 + DQZ_MAX_DEGREE + slot];
+      const int src = (int)(code & 3);
+      const cd *m = (src == DQZ_SRC_E2N_OLD ? e2n_old : (src == DQZ_SRC_N2E_NEW ? n2e_new : n2e_old)) + (code >> 2);
+      for (int x = lane; x < q2; x += 32) Ms[off + x] = m[x];
+      off += q2;
+      ++slot;
+    }
+    __syncwarp();
+  }
+  for (int a = 0; a < ce; ++a) {
+    for (unsigned x = lane; x < P; x += 32) {
+      const unsigned l = fRe.div(x), r = x - l * Re;
+      bufA[x] = Ts[(l * (unsigned)ce + (unsigned)a) * Re + r];
+    }
+    __syncwarp();
+    cd *cur = bufA, *nxt = bufB;
+    unsigned Lj = 1;
+    int off = 0;
+    for (int f = 0; f < k; ++f) {
+      if (f == e) continue;
+      const int q = (int)dims[f];
+      const unsigned R = P / Lj / (unsigned)q;
+      warp_mode_product(cur, nxt, Lj, q, R, Ms + off);
+      __syncwarp();
+      cd *t = cur;
+      cur = nxt;
+      nxt = t;
+      Lj *= (unsigned)q;
+      off += q * q;
+    }
+    for (int ap = 0; ap < ce; ++ap) {
+      cd acc = czero();
+      for (unsigned x = lane; x < P; x += 32) {
+        const unsigned l = fRe.div(x), r = x - l * Re;
+        cfmac(acc, Ts[(l * (unsigned)ce + (unsigned)ap) * Re + r], cur[x]);
+      }
+      acc = warp_csum(acc);
+      if (lane == 0) out[ap * ce + a] = acc;
+    }
+    __syncwarp();
+  }
+  cd tr = czero();
+  if (lane == 0)
+    for (int i = 0; i < ce; ++i) tr = cadd(tr, out[i * ce + i]);
+  tr.x = __shfl_sync(0xffffffffu, tr.x, 0);
+  tr.y = __shfl_sync(0xffffffffu, tr.y, 0);
+  cd *dst = n2e_new + pw[4];
+  for (int i = lane; i < ce * ce; i += 32) dst[i] = cdiv(out[i], tr);
+  __syncwarp();
+}
+
+__global__ void __launch_bounds__(ONECTA_THREADS) bp_sweep_planned_kernel(
+    dqz_graph_t g, const cd *__restrict__ T, const cd *n2e_old, const cd *e2n_old, cd *n2e_new, cd *e2n_new,
+    const uint8_t *__restrict__ edge_new, const long long *__restrict__ plan, const int32_t *__restrict__ level_off,
+    int n_levels, int max_slice, int max_chi) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5, lane = threadIdx.x & 31;
+  long long *pw = reinterpret_cast<long long *>(smem_raw) + (size_t)warp * DQZ_PLAN_WORDS;
+  cd *out = reinterpret_cast<cd *>(smem_raw + round_up16((size_t)nw * DQZ_PLAN_WORDS * sizeof(long long))) +
+            (size_t)warp * onecta_warp_elems(max_slice, max_chi);
+  cd *bufA = out + (size_t)max_chi * max_chi;
+  cd *bufB = bufA + max_slice;
+  cd *Ts = bufB + max_slice;
+  cd *Ms = Ts + (size_t)max_slice * max_chi;
+  for (int lv = 0; lv < n_levels; ++lv) {
+    for (int item = level_off[lv] + warp; item < level_off[lv + 1]; item += nw) {
+      if (lane < DQZ_PLAN_WORDS) pw[lane] = plan[(long long)item * DQZ_PLAN_WORDS + lane];
+      __syncwarp();
+      warp_plan_item(pw, T, n2e_old, e2n_old, n2e_new, out, bufA, bufB, Ts, Ms);
+    }
     __syncthreads();
   }
   for (int h = warp; h < g.n_halves; h += nw) {
@@ -592,6 +705,29 @@ extern "C" int dqz_bp_sweep_levels(const dqz_graph_t *g, const void *tensors, co
                          (int)n_levels, (int)max_slice, (int)max_chi, (unsigned *)sync, (int *)error_flag) !=
       cudaSuccess)
     return DQZ_ERR_CUDA;
+  return DQZ_OK;
+}
+
+extern "C" int dqz_bp_sweep_planned(const dqz_graph_t *g, const void *tensors, const void *n2e_old,
+                                    const void *e2n_old, void *n2e_new, void *e2n_new, const uint8_t *edge_new,
+                                    const int64_t *plan, const int32_t *level_off, int32_t n_levels,
+                                    int32_t max_level, int32_t max_slice, int32_t max_chi, cudaStream_t stream) {
+  if (!g || !tensors || !n2e_old || !e2n_old || !n2e_new || !e2n_new || !edge_new || !plan || !level_off ||
+      n_levels <= 0 || max_level <= 0 || max_slice <= 0)
+    return DQZ_ERR_ARG;
+  if (max_chi <= 0 || max_chi > DQZ_MAX_CHI) return DQZ_ERR_UNSUPPORTED;
+  const size_t per_warp = onecta_warp_elems(max_slice, max_chi) * sizeof(cd);
+  int warps = ONECTA_THREADS / 32;
+  while (warps > 8 && round_up16((size_t)warps * DQZ_PLAN_WORDS * sizeof(long long)) + warps * per_warp >
+                          BP_SMEM_LIMIT)
+    --warps;
+  const size_t smem = round_up16((size_t)warps * DQZ_PLAN_WORDS * sizeof(long long)) + warps * per_warp;
+  if (smem > BP_SMEM_LIMIT) return DQZ_ERR_UNSUPPORTED;
+  DQZ_SMEM_ATTR_ONCE(bp_sweep_planned_kernel, BP_SMEM_LIMIT);
+  bp_sweep_planned_kernel<<<1, 32 * warps, smem, stream>>>(
+      *g, (const cd *)tensors, (const cd *)n2e_old, (const cd *)e2n_old, (cd *)n2e_new, (cd *)e2n_new, edge_new,
+      (const long long *)plan, level_off, (int)n_levels, (int)max_slice, (int)max_chi);
+  DQZ_CHECK_LAUNCH();
   return DQZ_OK;
 }
 

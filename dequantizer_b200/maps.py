@@ -174,6 +174,44 @@ class Topology:
                           torch.from_numpy(np.array(off, dtype=np.int32)).to(device), widest)
         return cache[key]
 
+    def device_plan(self, layout, device):
+        """The plan of the one-CTA sweep (dqz_bp_sweep_planned): per half-edge of
+        the flat level table, node offset, degree, physical dimension, slot,
+        outgoing message offset, bond dimensions, and the incoming messages as
+        offset * 4 + source, from the layout's current bond dimensions."""
+        key = layout.edge_chi.tobytes()
+        cache = self.__dict__.setdefault("_dev_plan", {})
+        if key not in cache:
+            H = (np.concatenate(self.levels) if self.levels else np.zeros(0, np.int32)).astype(np.int64)
+            v = layout.half_node[H].astype(np.int64)
+            h0 = layout.node_half[v].astype(np.int64)
+            k = layout.degree[v].astype(np.int64)
+            md = _lib.MAX_DEGREE
+            plan = np.zeros((len(H), _lib.PLAN_WORDS), dtype=np.int64)
+            plan[:, 0] = layout.node_off[v]
+            plan[:, 1] = k
+            plan[:, 2] = layout.phys[v]
+            plan[:, 3] = H - h0
+            plan[:, 4] = layout.half_msg_off[H]
+            slot = np.zeros(len(H), dtype=np.int64)
+            twin = layout.half_twin
+            for j in range(md):
+                has = j < k
+                hf = np.where(has, h0 + j, 0)
+                he = layout.half_edge[hf]
+                plan[:, 5 + j] = np.where(has, layout.edge_chi[np.maximum(he, 0)], 0)
+                other = has & (j != plan[:, 3])
+                sel = self.src_sel[hf].astype(np.int64)
+                off = np.where(sel == _lib.SRC_E2N_OLD, layout.half_msg_off[hf],
+                               layout.half_msg_off[np.maximum(twin[hf], 0)])
+                rows = np.nonzero(other)[0]
+                plan[rows, 5 + md + slot[rows]] = off[rows] * 4 + sel[rows]
+                slot += other
+            if len(cache) > 8:
+                cache.clear()
+            cache[key] = torch.from_numpy(plan).to(device)
+        return cache[key]
+
     def device_node_levels(self, device):
         if self._dev_nodes is None:
             self._dev_nodes = [torch.from_numpy(l).to(device) for l in self.node_levels]
@@ -277,6 +315,13 @@ def bp_sweep(layout: GraphLayout, topo: Topology, T, n2e_old, e2n_old, n2e_new, 
                 e2n_new.data_ptr(), src_sel.data_ptr(), edge_new.data_ptr(), flat.data_ptr(), off.data_ptr(),
                 ih.data_ptr(), isl.data_ptr(), ioff.data_ptr(), len(topo.levels), widest_items, max_slice, max_chi,
                 sync.data_ptr(), error_flag(layout.device).data_ptr(), stream)
+        elif max_slice <= 256 and widest <= 64 and _lib.lib().dqz_get_tuning(_lib.TUNE_SWEEP_ONECTA) == 0:
+            # small nodes and narrow levels: one CTA, a warp per half-edge, driven by the plan
+            # (knob sweep_onecta: 1 = the cooperative grid, 2 = the one-CTA form without a plan)
+            status = _lib.lib().dqz_bp_sweep_planned(
+                layout.gptr, T.data_ptr(), n2e_old.data_ptr(), e2n_old.data_ptr(), n2e_new.data_ptr(),
+                e2n_new.data_ptr(), edge_new.data_ptr(), topo.device_plan(layout, layout.device).data_ptr(),
+                off.data_ptr(), len(topo.levels), widest, max_slice, max_chi, stream)
         else:
             status = _lib.lib().dqz_bp_sweep_levels(
                 layout.gptr, T.data_ptr(), n2e_old.data_ptr(), e2n_old.data_ptr(), n2e_new.data_ptr(),

@@ -168,6 +168,23 @@ int dqz_bp_sweep_levels(const dqz_graph_t *g, const void *tensors, const void *n
                         int32_t max_slice, int32_t max_chi, uint32_t *sync, int32_t *error_flag,
                         cudaStream_t stream);
 
+/* The one-CTA form of dqz_bp_sweep_levels driven by a host-built plan, one
+ * entry of DQZ_PLAN_WORDS int64 words per item in the order of the level
+ * table (level l: items level_off[l] .. level_off[l+1]): node tensor offset,
+ * degree k, physical dimension d, slot e of the outgoing bond, outgoing
+ * message offset (half_msg_off of the item's half-edge), the bond dimensions
+ * (DQZ_MAX_DEGREE words, the first k used), then for every other bond in bond
+ * order its incoming message as offset * 4 + source (DQZ_SRC_*: the offset
+ * into e2n_old, n2e_old or n2e_new). A warp per item, a CTA barrier between
+ * levels, then the edge pass; the same results as dqz_bp_sweep_levels, bit
+ * for bit. DQZ_ERR_UNSUPPORTED when a warp's buffers (two bond slices, the
+ * node tensor, its messages) do not fit in shared memory eight times. */
+#define DQZ_PLAN_WORDS (5 + DQZ_MAX_DEGREE + DQZ_MAX_DEGREE - 1)
+int dqz_bp_sweep_planned(const dqz_graph_t *g, const void *tensors, const void *n2e_old, const void *e2n_old,
+                         void *n2e_new, void *e2n_new, const uint8_t *edge_new, const int64_t *plan,
+                         const int32_t *level_off, int32_t n_levels, int32_t max_level, int32_t max_slice,
+                         int32_t max_chi, cudaStream_t stream);
+
 /* The same sweep for large bonds: the work items of level l are
  * (item_half[i], item_slice[i]) for i in item_off[l] .. item_off[l+1] (every
  * slice of the bond of every half-edge of the level), spread over the grid;

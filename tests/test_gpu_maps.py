@@ -424,14 +424,16 @@ def test_gauge_knobs_leave_results_unchanged_and_tuner_caches(tmp_path):
         autotune.set_knobs({k: 0 for k in autotune.KNOBS})
 
 
-@pytest.mark.parametrize("case,onecta", [("lattice_3x3x3", 0), ("lattice_3x3x3", 1), ("eagle_cell_4", 0),
-                                         ("eagle_cell_4", 1), ("eagle_cell_8_16", 0), ("eagle_cell_32", 0)])
+@pytest.mark.parametrize("case,onecta", [("lattice_3x3x3", 0), ("lattice_3x3x3", 1), ("lattice_3x3x3", 2),
+                                         ("eagle_cell_4", 0), ("eagle_cell_4", 1), ("eagle_cell_4", 2),
+                                         ("eagle_cell_8_16", 0), ("eagle_cell_32", 0)])
 def test_one_launch_sweep_equals_level_launches(case, onecta):
     """The one-launch asynchronous sweep (every node level of the DFS schedule
     and the edge pass in one launch: below bond 8 one CTA with a warp per
-    half-edge and CTA barriers between levels (small nodes, the default) or a
-    cooperative grid with grid barriers (dqz_bp_sweep_levels, knob
-    sweep_onecta = 1); from bond 8 dqz_bp_sweep_sliced with one work item per
+    half-edge and CTA barriers between levels (small nodes: driven by a host
+    plan, dqz_bp_sweep_planned, the default; or walking the graph tables,
+    knob sweep_onecta = 2) or a cooperative grid with grid barriers
+    (dqz_bp_sweep_levels, knob sweep_onecta = 1); from bond 8 dqz_bp_sweep_sliced with one work item per
     bond slice) gives one dqz_bp_node_update launch per level plus
     dqz_bp_edge_pass, bit for bit, over several sweeps; mixed bonds of 8 and
     16 give levels of uneven item counts."""

@@ -225,3 +225,36 @@ def test_layout_pack_roundtrip_on_host():
             assert L.edges[L.half_edge[h]] is e
             tw = L.half_twin[h]
             assert L.half_edge[tw] == L.half_edge[h] and L.half_node[tw] != v
+
+
+@pytest.mark.parametrize("make", [lambda: G.get_nd_lattice([3, 3, 2], 2, 2),
+                                  lambda: G.get_heavy_hex_ibm_eagle_lattice_infinite()])
+def test_sweep_plan_matches_layout_tables(make):
+    """The host plan of the one-CTA sweep (dqz_bp_sweep_planned): for every
+    item of the flat level table, the node offset, degree, physical
+    dimension, slot, outgoing message offset, bond dimensions and, per other
+    bond in order, the incoming message as offset * 4 + source, as the
+    kernels that walk the graph tables would find them."""
+    g = make()
+    topo = Topology(list(g.get_traversal_iterator(ordering="dfs")), is_synchronous=False)
+    L = GraphLayout(topo.nodes, topo.edges, [e.dimension for e in topo.edges], device=torch.device("cpu"))
+    plan = topo.device_plan(L, torch.device("cpu")).numpy()
+    flat = np.concatenate(topo.levels)
+    assert plan.shape == (len(flat), _lib.PLAN_WORDS)
+    for i, h in enumerate(flat):
+        v = int(L.half_node[h])
+        h0, k = int(L.node_half[v]), int(L.degree[v])
+        row = plan[i]
+        assert row[0] == L.node_off[v] and row[1] == k and row[2] == L.phys[v] and row[3] == h - h0
+        assert row[4] == L.half_msg_off[h]
+        for j in range(k):
+            assert row[5 + j] == L.edge_chi[L.half_edge[h0 + j]]
+        slot = 0
+        for j in range(k):
+            if j == h - h0:
+                continue
+            hf = h0 + j
+            sel = int(topo.src_sel[hf])
+            off = L.half_msg_off[hf] if sel == _lib.SRC_E2N_OLD else L.half_msg_off[L.half_twin[hf]]
+            assert row[5 + _lib.MAX_DEGREE + slot] == off * 4 + sel
+            slot += 1
