@@ -146,12 +146,13 @@ __global__ void __launch_bounds__(BP_THREADS) bp_node_generic(dqz_graph_t g, con
 // the messages are bit-identical; phases are separated by __syncwarp only.
 __device__ __forceinline__ void warp_mode_product(const cd *__restrict__ X, cd *__restrict__ Y, unsigned L, int q,
                                                   unsigned R, const cd *__restrict__ m) {
+  // plain 32-bit divisions: a lane runs a handful of outputs here (small
+  // nodes), fewer than it takes to amortise a FastDiv set-up
   const unsigned total = L * (unsigned)q * R;
-  const FastDiv fR(R), fq((unsigned)q);
   for (unsigned o = threadIdx.x & 31; o < total; o += 32) {
-    const unsigned t = fR.div(o);
+    const unsigned t = o / R;
     const unsigned r = o - t * R;
-    const unsigned l = fq.div(t);
+    const unsigned l = t / (unsigned)q;
     const int i = (int)(t - l * (unsigned)q);
     const cd *x = X + (l * (unsigned)q) * R + r;
     cd acc = czero();
@@ -291,7 +292,6 @@ __device__ __forceinline__ void warp_plan_item(const long long *pw, const cd *__
   }
   const int ce = (int)dims[e];
   const unsigned P = size / (unsigned)ce;
-  const FastDiv fRe(Re);
   {
     const cd *Tv = T + pw[0];
     for (unsigned x = lane; x < size; x += 32) Ts[x] = Tv[x];
@@ -310,7 +310,7 @@ __device__ __forceinline__ void warp_plan_item(const long long *pw, const cd *__
   }
   for (int a = 0; a < ce; ++a) {
     for (unsigned x = lane; x < P; x += 32) {
-      const unsigned l = fRe.div(x), r = x - l * Re;
+      const unsigned l = x / Re, r = x - l * Re;
       bufA[x] = Ts[(l * (unsigned)ce + (unsigned)a) * Re + r];
     }
     __syncwarp();
@@ -332,7 +332,7 @@ __device__ __forceinline__ void warp_plan_item(const long long *pw, const cd *__
     for (int ap = 0; ap < ce; ++ap) {
       cd acc = czero();
       for (unsigned x = lane; x < P; x += 32) {
-        const unsigned l = fRe.div(x), r = x - l * Re;
+        const unsigned l = x / Re, r = x - l * Re;
         cfmac(acc, Ts[(l * (unsigned)ce + (unsigned)ap) * Re + r], cur[x]);
       }
       acc = warp_csum(acc);
