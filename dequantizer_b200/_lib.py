@@ -82,8 +82,6 @@ _SIGNATURES = {
     "dqz_bp_node_scratch_bytes": (_S, [_I, _I, _I]),
     "dqz_bp_edge_pass": (ctypes.c_int, [_G, _P, _P, _P, _P, _I, _P]),
     "dqz_bp_sweep_levels": (ctypes.c_int, [_G, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I, _I, _I, _I, _P, _P, _P]),
-    "dqz_bp_sweep_split": (ctypes.c_int, [_G, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P,
-                                          _I, _I, _I, _I, _I, _P, _P, _P, _P, _P]),
     "dqz_bp_sweep_planned": (ctypes.c_int, [_G, _P, _P, _P, _P, _P, _P, _P, _P, _I, _I, _I, _I, _P]),
     "dqz_bp_sweep_sliced": (ctypes.c_int, [_G, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I, _I, _I, _I, _P, _P,
                                            _P]),

@@ -503,145 +503,6 @@ __global__ void __launch_bounds__(SLICED_THREADS) bp_sweep_sliced_kernel(
   }
 }
 
-// ---- the sweep for large bonds, with the final contraction split over x
-// (the entries of a bond slice) instead of re-reading the node tensor per
-// slice. Per level: (A) every (half-edge h, slice a) item contracts slice a
-// with the incoming messages (as node_slice_column does) and writes Y_a to a
-// global scratch (L2-resident); (B) every (h, chunk c) item forms the partial
-// out[a'][a] = sum over the chunk's x of conj(T_a'[x]) Y_a[x], the chunk of T
-// and of every Y_a staged in shared memory (the node tensor is read once per
-// half-edge, not once per slice); (C) every h sums its chunks in chunk order,
-// divides by the trace and writes the message. Three grid barriers a level.
-// The same messages up to the summation order of the final contraction.
-__device__ __forceinline__ cd *node_slice_contract(const dqz_graph_t &g, const cd *__restrict__ Tv,
-                                                   const NodeShape &s, int e, const cd *n2e_old, const cd *e2n_old,
-                                                   const cd *n2e_new, const uint8_t *__restrict__ src_sel, int a,
-                                                   cd *bufA, cd *bufB) {
-  const int ce = s.dims[e];
-  const unsigned Re = (unsigned)s.stride[e];
-  const unsigned P = (unsigned)(s.size / ce);
-  const FastDiv fRe(Re);
-  for (unsigned x = threadIdx.x; x < P; x += blockDim.x) {
-    const unsigned l = fRe.div(x), r = x - l * Re;
-    bufA[x] = Tv[(l * (unsigned)ce + (unsigned)a) * Re + r];
-  }
-  __syncthreads();
-  cd *cur = bufA, *nxt = bufB;
-  long long Lj = 1;
-  for (int f = 0; f < s.k; ++f) {
-    if (f == e) continue;
-    const int q = s.dims[f];
-    const long long R = (long long)P / Lj / q;
-    const cd *m = incoming_msg(g, s.half0 + f, n2e_old, e2n_old, n2e_new, src_sel);
-    mode_product<false>(cur, nxt, Lj, q, q, R, m, q, 1);
-    __syncthreads();
-    cd *t = cur;
-    cur = nxt;
-    nxt = t;
-    Lj *= q;
-  }
-  return cur;
-}
-
-__global__ void __launch_bounds__(SLICED_THREADS) bp_sweep_split_kernel(
-    dqz_graph_t g, const cd *__restrict__ T, const cd *n2e_old, const cd *e2n_old, cd *n2e_new, cd *e2n_new,
-    const uint8_t *__restrict__ src_sel, const uint8_t *__restrict__ edge_new, const int32_t *__restrict__ halves,
-    const int32_t *__restrict__ level_off, const int32_t *__restrict__ item_half,
-    const int32_t *__restrict__ item_slice, const int32_t *__restrict__ item_off,
-    const int32_t *__restrict__ chunk_half, const int32_t *__restrict__ chunk_id,
-    const int32_t *__restrict__ chunk_off, const int64_t *__restrict__ half_ybase,
-    const int64_t *__restrict__ half_pbase, int n_levels, int max_slice, int max_chi, int xc, cd *Y, cd *part,
-    unsigned *sync, int *error_flag) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  cd *out = reinterpret_cast<cd *>(smem_raw + 48 * sizeof(double));
-  cd *bufA = out + (long long)max_chi * max_chi;
-  cd *bufB = bufA + max_slice;
-  __shared__ cd trace_sh;
-  const int tid = threadIdx.x, nt = blockDim.x;
-  unsigned gen = 0;
-  for (int lv = 0; lv < n_levels; ++lv) {
-    // (A) contracted slices
-    for (int item = item_off[lv] + blockIdx.x; item < item_off[lv + 1]; item += gridDim.x) {
-      const int h = item_half[item], a = item_slice[item];
-      const int v = g.half_node[h];
-      NodeShape s;
-      load_shape(g, v, s);
-      const int e = h - s.half0;
-      const int ce = s.dims[e];
-      const long long P = s.size / ce;
-      const cd *cur = node_slice_contract(g, T + g.node_off[v], s, e, n2e_old, e2n_old, n2e_new, src_sel, a, bufA,
-                                          bufB);
-      cd *ya = Y + half_ybase[h] + (long long)a * P;
-      for (long long x = tid; x < P; x += nt) ya[x] = cur[x];
-      __syncthreads();
-    }
-    if (!grid_barrier(sync, gen, error_flag)) return;
-    // (B) partial final contractions over chunks of x
-    for (int item = chunk_off[lv] + blockIdx.x; item < chunk_off[lv + 1]; item += gridDim.x) {
-      const int h = chunk_half[item], c = chunk_id[item];
-      const int v = g.half_node[h];
-      NodeShape s;
-      load_shape(g, v, s);
-      const int e = h - s.half0;
-      const int ce = s.dims[e];
-      const unsigned Re = (unsigned)s.stride[e];
-      const unsigned P = (unsigned)(s.size / ce);
-      const unsigned x0 = (unsigned)c * (unsigned)xc;
-      const int nx = (int)((P - x0) < (unsigned)xc ? (P - x0) : (unsigned)xc);
-      const FastDiv fRe(Re);
-      const cd *Tv = T + g.node_off[v];
-      const cd *Yh = Y + half_ybase[h];
-      // Ts[a'][xl] = T_a'[x0 + xl]; Ys[xl][a] = Y_a[x0 + xl] (a fastest: conflict-free reads below)
-      for (int idx = tid; idx < ce * nx; idx += nt) {
-        const int ap = idx / nx, xl = idx - ap * nx;
-        const unsigned x = x0 + (unsigned)xl;
-        const unsigned l = fRe.div(x), r = x - l * Re;
-        bufA[idx] = Tv[(l * (unsigned)ce + (unsigned)ap) * Re + r];
-        bufB[xl * ce + ap] = Yh[(long long)ap * P + x];
-      }
-      __syncthreads();
-      cd *pc = part + half_pbase[h] + (long long)c * ce * ce;
-      for (int o = tid; o < ce * ce; o += nt) {
-        const int ap = o / ce, a = o - ap * ce;
-        cd acc = czero();
-        for (int xl = 0; xl < nx; ++xl) cfmac(acc, bufA[ap * nx + xl], bufB[xl * ce + a]);
-        pc[o] = acc;
-      }
-      __syncthreads();
-    }
-    if (!grid_barrier(sync, gen, error_flag)) return;
-    // (C) chunks summed in order, divided by the trace
-    for (int i = level_off[lv] + blockIdx.x; i < level_off[lv + 1]; i += gridDim.x) {
-      const int h = halves[i];
-      const int v = g.half_node[h];
-      NodeShape s;
-      load_shape(g, v, s);
-      const int ce = s.dims[h - s.half0];
-      const long long P = s.size / ce;
-      const int nch = (int)((P + xc - 1) / xc);
-      const cd *ph = part + half_pbase[h];
-      for (int o = tid; o < ce * ce; o += nt) {
-        cd acc = ph[o];
-        for (int c = 1; c < nch; ++c) acc = cadd(acc, ph[(long long)c * ce * ce + o]);
-        out[o] = acc;
-      }
-      __syncthreads();
-      normalise_by_trace(out, n2e_new + g.half_msg_off[h], ce, trace_sh);
-    }
-    if (!grid_barrier(sync, gen, error_flag)) return;
-  }
-  const int wpb = blockDim.x >> 5;
-  for (int h = blockIdx.x * wpb + (threadIdx.x >> 5); h < g.n_halves; h += gridDim.x * wpb) {
-    const int e = g.half_edge[h];
-    const int tw = g.half_twin[h];
-    if (e < 0 || tw < 0) continue;
-    const int c = g.edge_chi[e];
-    const cd *src = (edge_new[h] ? n2e_new : n2e_old) + g.half_msg_off[tw];
-    cd *dst = e2n_new + g.half_msg_off[h];
-    warp_copy16(reinterpret_cast<uint4 *>(dst), reinterpret_cast<const uint4 *>(src), c * c);
-  }
-}
-
 __global__ void bp_edge_pass_kernel(dqz_graph_t g, const cd *n2e_old, const cd *n2e_new,
                                     const uint8_t *__restrict__ edge_new, cd *e2n_new) {
   const int nh = g.n_halves;
@@ -867,52 +728,6 @@ extern "C" int dqz_bp_sweep_planned(const dqz_graph_t *g, const void *tensors, c
       *g, (const cd *)tensors, (const cd *)n2e_old, (const cd *)e2n_old, (cd *)n2e_new, (cd *)e2n_new, edge_new,
       (const long long *)plan, level_off, (int)n_levels, (int)max_slice, (int)max_chi);
   DQZ_CHECK_LAUNCH();
-  return DQZ_OK;
-}
-
-extern "C" int dqz_bp_sweep_split(const dqz_graph_t *g, const void *tensors, const void *n2e_old,
-                                  const void *e2n_old, void *n2e_new, void *e2n_new, const uint8_t *src_sel,
-                                  const uint8_t *edge_new, const int32_t *halves, const int32_t *level_off,
-                                  const int32_t *item_half, const int32_t *item_slice, const int32_t *item_off,
-                                  const int32_t *chunk_half, const int32_t *chunk_id, const int32_t *chunk_off,
-                                  const int64_t *half_ybase, const int64_t *half_pbase, int32_t n_levels,
-                                  int32_t max_items, int32_t max_slice, int32_t max_chi, int32_t xc, void *Y,
-                                  void *part, uint32_t *sync, int32_t *error_flag, cudaStream_t stream) {
-  if (!g || !tensors || !n2e_old || !e2n_old || !n2e_new || !e2n_new || !src_sel || !edge_new || !halves ||
-      !level_off || !item_half || !item_slice || !item_off || !chunk_half || !chunk_id || !chunk_off ||
-      !half_ybase || !half_pbase || !Y || !part || !sync || !error_flag || n_levels <= 0 || max_items <= 0 ||
-      max_slice <= 0 || xc <= 0)
-    return DQZ_ERR_ARG;
-  if (max_chi <= 0 || max_chi > DQZ_MAX_CHI || (long long)xc * max_chi > max_slice) return DQZ_ERR_UNSUPPORTED;
-  const size_t smem = bp_smem_bytes(max_slice, max_chi, false);
-  if (smem > BP_SMEM_LIMIT) return DQZ_ERR_UNSUPPORTED;
-  DQZ_SMEM_ATTR_ONCE(bp_sweep_split_kernel, BP_SMEM_LIMIT);
-  int dev = 0, sms = 148, per_sm = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess) return DQZ_ERR_CUDA;
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bp_sweep_split_kernel, SLICED_THREADS, smem) !=
-          cudaSuccess ||
-      per_sm < 1)
-    return DQZ_ERR_UNSUPPORTED;
-  int grid = max_items;
-  if (grid > sms * per_sm) grid = sms * per_sm;
-  if (cudaMemsetAsync(sync, 0, 2 * sizeof(uint32_t), stream) != cudaSuccess) return DQZ_ERR_CUDA;
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(grid);
-  cfg.blockDim = dim3(SLICED_THREADS);
-  cfg.dynamicSmemBytes = smem;
-  cfg.stream = stream;
-  cudaLaunchAttribute attr[1];
-  attr[0].id = cudaLaunchAttributeCooperative;
-  attr[0].val.cooperative = 1;
-  cfg.attrs = attr;
-  cfg.numAttrs = 1;
-  if (cudaLaunchKernelEx(&cfg, bp_sweep_split_kernel, *g, (const cd *)tensors, (const cd *)n2e_old,
-                         (const cd *)e2n_old, (cd *)n2e_new, (cd *)e2n_new, src_sel, edge_new, halves, level_off,
-                         item_half, item_slice, item_off, chunk_half, chunk_id, chunk_off, half_ybase, half_pbase,
-                         (int)n_levels, (int)max_slice, (int)max_chi, (int)xc, (cd *)Y, (cd *)part,
-                         (unsigned *)sync, (int *)error_flag) != cudaSuccess)
-    return DQZ_ERR_CUDA;
   return DQZ_OK;
 }
 

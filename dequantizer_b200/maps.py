@@ -174,43 +174,6 @@ class Topology:
                           torch.from_numpy(np.array(off, dtype=np.int32)).to(device), widest)
         return cache[key]
 
-    def device_split_items(self, layout, device, xc: int):
-        """Tables of the split large-bond sweep (dqz_bp_sweep_split) for the
-        layout's current bond dimensions and chunk width xc: the (half-edge,
-        chunk) items of every level with offsets, each half-edge's offsets into
-        the contracted-slice scratch Y and the partial scratch (restarting at
-        every level), the scratch sizes (complex entries) and the largest item
-        count of any phase of a level."""
-        key = (layout.edge_chi.tobytes(), int(xc))
-        cache = self.__dict__.setdefault("_dev_split", {})
-        if key not in cache:
-            he = layout.half_edge
-            ce = np.where(he >= 0, layout.edge_chi[np.maximum(he, 0)], 0).astype(np.int64)
-            size = layout.node_sizes()[layout.half_node].astype(np.int64)
-            P = size // np.maximum(ce, 1)
-            nch = (P + xc - 1) // xc
-            ybase = np.zeros(layout.n_halves, dtype=np.int64)
-            pbase = np.zeros(layout.n_halves, dtype=np.int64)
-            ch_h, ch_c, off = [], [], [0]
-            y_max = p_max = 0
-            widest = 0
-            for lv in self.levels:
-                lv = lv.astype(np.int64)
-                ysz, psz = size[lv], nch[lv] * ce[lv] * ce[lv]
-                ybase[lv] = np.concatenate([[0], np.cumsum(ysz)[:-1]])
-                pbase[lv] = np.concatenate([[0], np.cumsum(psz)[:-1]])
-                y_max, p_max = max(y_max, int(ysz.sum())), max(p_max, int(psz.sum()))
-                ch_h.append(np.repeat(lv, nch[lv]))
-                ch_c.append(np.concatenate([np.arange(n) for n in nch[lv]]) if len(lv) else np.zeros(0, np.int64))
-                off.append(off[-1] + int(nch[lv].sum()))
-                widest = max(widest, int(nch[lv].sum()), int(ce[lv].sum()), len(lv))
-            t = lambda a, dt: torch.from_numpy(np.asarray(a, dtype=dt)).to(device)
-            if len(cache) > 8:
-                cache.clear()
-            cache[key] = (t(np.concatenate(ch_h), np.int32), t(np.concatenate(ch_c), np.int32), t(off, np.int32),
-                          t(ybase, np.int64), t(pbase, np.int64), y_max, p_max, widest)
-        return cache[key]
-
     def device_plan(self, layout, device):
         """The plan of the one-CTA sweep (dqz_bp_sweep_planned): per half-edge of
         the flat level table, node offset, degree, physical dimension, slot,
@@ -291,9 +254,6 @@ BF16_KERNELS = {"tcgen05": "dqz_bp_node_update_k3_umma", "mma_sync": "dqz_bp_nod
 # half-edges) over the grid: at bond 32 a level of the heavy-hex DFS schedule
 # has a handful of half-edges of ~50 MFLOP each
 SLICED_MIN_CHI = 8
-# large-bond asynchronous sweep: "split" (dqz_bp_sweep_split, the default) or
-# "sliced" (dqz_bp_sweep_sliced, bit-identical to the per-level launches)
-LARGE_BOND_SWEEP = "split"
 
 
 def bp_sweep(layout: GraphLayout, topo: Topology, T, n2e_old, e2n_old, n2e_new, e2n_new, mid_event=None,
@@ -346,21 +306,7 @@ def bp_sweep(layout: GraphLayout, topo: Topology, T, n2e_old, e2n_old, n2e_new, 
         # a schedule of several node levels (the reference's asynchronous sweep):
         # all levels and the edge pass in one launch when a slice fits on chip
         flat, off, widest, sync = topo.device_level_tables(layout.device)
-        if max_chi >= SLICED_MIN_CHI and LARGE_BOND_SWEEP == "split":
-            # large bonds: the slices' contractions, then the final contraction split
-            # over chunks of the slice entries (the node tensor read once per half-edge)
-            ih, isl, ioff, _ = topo.device_slice_items(layout, layout.device)
-            xc = max(1, max_slice // max_chi)
-            ch, cc, coff, yb, pb, y_n, p_n, widest_items = topo.device_split_items(layout, layout.device, xc)
-            Y = torch.empty(max(y_n, 1), dtype=torch.complex128, device=layout.device)
-            part = torch.empty(max(p_n, 1), dtype=torch.complex128, device=layout.device)
-            status = _lib.lib().dqz_bp_sweep_split(
-                layout.gptr, T.data_ptr(), n2e_old.data_ptr(), e2n_old.data_ptr(), n2e_new.data_ptr(),
-                e2n_new.data_ptr(), src_sel.data_ptr(), edge_new.data_ptr(), flat.data_ptr(), off.data_ptr(),
-                ih.data_ptr(), isl.data_ptr(), ioff.data_ptr(), ch.data_ptr(), cc.data_ptr(), coff.data_ptr(),
-                yb.data_ptr(), pb.data_ptr(), len(topo.levels), widest_items, max_slice, max_chi, xc, Y.data_ptr(),
-                part.data_ptr(), sync.data_ptr(), error_flag(layout.device).data_ptr(), stream)
-        elif max_chi >= SLICED_MIN_CHI:
+        if max_chi >= SLICED_MIN_CHI:
             # large bonds: every (half-edge, slice) of a level is a work item, so a
             # level of a few half-edges still spreads over the whole GPU
             ih, isl, ioff, widest_items = topo.device_slice_items(layout, layout.device)

@@ -198,28 +198,6 @@ int dqz_bp_sweep_sliced(const dqz_graph_t *g, const void *tensors, const void *n
                         int32_t max_slice, int32_t max_chi, uint32_t *sync, int32_t *error_flag,
                         cudaStream_t stream);
 
-/* The large-bond sweep with the final contraction split over the entries of
- * a bond slice: per level, (A) the (half-edge, slice) items of
- * item_off[l] .. item_off[l+1] write the slice contracted with the incoming
- * messages to Y (at half_ybase[h] + slice * slice size), (B) the
- * (half-edge, chunk) items of chunk_off[l] .. chunk_off[l+1] (chunk c covers
- * slice entries c*xc .. c*xc+xc-1) write partial outgoing messages to part
- * (at half_pbase[h] + c * chi^2), (C) each half-edge of the level sums its
- * chunks in order and divides by the trace; grid barriers in between, the
- * edge pass at the end. The node tensor is read once per half-edge instead of
- * once per slice. The same messages as dqz_bp_sweep_sliced up to the
- * summation order of the final contraction. Y and part hold the largest
- * level's needs (the offsets restart at every level); xc * max_chi <=
- * max_slice; max_items bounds the items of any phase of a level. */
-int dqz_bp_sweep_split(const dqz_graph_t *g, const void *tensors, const void *n2e_old, const void *e2n_old,
-                       void *n2e_new, void *e2n_new, const uint8_t *src_sel, const uint8_t *edge_new,
-                       const int32_t *halves, const int32_t *level_off, const int32_t *item_half,
-                       const int32_t *item_slice, const int32_t *item_off, const int32_t *chunk_half,
-                       const int32_t *chunk_id, const int32_t *chunk_off, const int64_t *half_ybase,
-                       const int64_t *half_pbase, int32_t n_levels, int32_t max_items, int32_t max_slice,
-                       int32_t max_chi, int32_t xc, void *Y, void *part, uint32_t *sync, int32_t *error_flag,
-                       cudaStream_t stream);
-
 /* Edge pass on complex64 messages (see dqz_bp_edge_pass). */
 int dqz_bp_edge_pass_c64(const dqz_graph_t *g, const void *n2e_old, const void *n2e_new,
                          const uint8_t *edge_new, void *e2n_new, cudaStream_t stream);

@@ -426,34 +426,28 @@ def test_gauge_knobs_leave_results_unchanged_and_tuner_caches(tmp_path):
 
 @pytest.mark.parametrize("case,onecta", [("lattice_3x3x3", 0), ("lattice_3x3x3", 1), ("lattice_3x3x3", 2),
                                          ("eagle_cell_4", 0), ("eagle_cell_4", 1), ("eagle_cell_4", 2),
-                                         ("eagle_cell_8_16", "sliced"), ("eagle_cell_32", "sliced"),
-                                         ("eagle_cell_8_16", "split"), ("eagle_cell_32", "split")])
+                                         ("eagle_cell_8_16", 0), ("eagle_cell_32", 0)])
 def test_one_launch_sweep_equals_level_launches(case, onecta):
     """The one-launch asynchronous sweep (every node level of the DFS schedule
     and the edge pass in one launch: below bond 8 one CTA with a warp per
     half-edge and CTA barriers between levels (small nodes: driven by a host
     plan, dqz_bp_sweep_planned, the default; or walking the graph tables,
     knob sweep_onecta = 2) or a cooperative grid with grid barriers
-    (dqz_bp_sweep_levels, knob sweep_onecta = 1); from bond 8 a work item per
-    bond slice, dqz_bp_sweep_sliced) gives one dqz_bp_node_update launch per
-    level plus dqz_bp_edge_pass, bit for bit, over several sweeps; the split
-    large-bond sweep (dqz_bp_sweep_split, the final contraction summed over
-    chunks of the slice entries) agrees to 1e-13 relative. Mixed bonds of 8
-    and 16 give levels of uneven item counts."""
+    (dqz_bp_sweep_levels, knob sweep_onecta = 1); from bond 8 dqz_bp_sweep_sliced with one work item per
+    bond slice) gives one dqz_bp_node_update launch per level plus
+    dqz_bp_edge_pass, bit for bit, over several sweeps; mixed bonds of 8 and
+    16 give levels of uneven item counts."""
     from dequantizer_b200 import _lib, autotune
     from dequantizer_b200.layout import GraphLayout
 
-    large = onecta if isinstance(onecta, str) else M.LARGE_BOND_SWEEP
-    autotune.set_knobs({"sweep_onecta": onecta if isinstance(onecta, int) else 0})
-    prev, M.LARGE_BOND_SWEEP = M.LARGE_BOND_SWEEP, large
+    autotune.set_knobs({"sweep_onecta": onecta})
     try:
-        _one_launch_sweep_case(case, exact=(large == "sliced"))
+        _one_launch_sweep_case(case)
     finally:
         autotune.set_knobs({"sweep_onecta": 0})
-        M.LARGE_BOND_SWEEP = prev
 
 
-def _one_launch_sweep_case(case, exact=True):
+def _one_launch_sweep_case(case):
     from dequantizer_b200 import _lib
     from dequantizer_b200.layout import GraphLayout
 
@@ -495,11 +489,7 @@ def _one_launch_sweep_case(case, exact=True):
                       src_sel.data_ptr(), halves.data_ptr(), halves.numel(), L.max_slice(), L.max_chi(), None, stream)
         _lib.call("dqz_bp_edge_pass", L.gptr, b[0].data_ptr(), nb.data_ptr(), edge_new.data_ptr(), eb.data_ptr(),
                   L.max_chi(), stream)
-        if exact or L.max_chi() < M.SLICED_MIN_CHI:
-            torch.cuda.synchronize()
-            assert torch.equal(na, nb) and torch.equal(ea, eb)
-        else:
-            # the split sweep sums the final contraction in another order
-            assert rel_err(na, nb) < 1e-13 and rel_err(ea, eb) < 1e-13
         a, b = (na, ea), (nb, eb)
+        torch.cuda.synchronize()
+        assert torch.equal(a[0], b[0]) and torch.equal(a[1], b[1])
     assert int(M.error_flag(T.device).item()) == 0

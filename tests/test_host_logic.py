@@ -258,39 +258,3 @@ def test_sweep_plan_matches_layout_tables(make):
             off = L.half_msg_off[hf] if sel == _lib.SRC_E2N_OLD else L.half_msg_off[L.half_twin[hf]]
             assert row[5 + _lib.MAX_DEGREE + slot] == off * 4 + sel
             slot += 1
-
-
-def test_split_sweep_tables_cover_each_level_without_overlap():
-    """dqz_bp_sweep_split's host tables on the heavy-hex cell with bonds of 8,
-    16 and 32: per level, each half-edge's contracted slices (node size) and
-    partials (chunks x chi^2) get disjoint scratch ranges inside the reported
-    sizes, and the chunk items of a half-edge are 0 .. ceil(slice / xc) - 1."""
-    g = G.get_heavy_hex_ibm_eagle_lattice_infinite()
-    rng = np.random.default_rng(3)
-    for e in g.edges.values():
-        e.dimension = int(rng.choice([8, 16, 32]))
-    g.refresh_bond_shapes()
-    topo = Topology(list(g.get_traversal_iterator(ordering="dfs")), is_synchronous=False)
-    L = GraphLayout(topo.nodes, topo.edges, [e.dimension for e in topo.edges], device=torch.device("cpu"))
-    xc = max(1, L.max_slice() // L.max_chi())
-    ch, cc, coff, yb, pb, y_n, p_n, widest = topo.device_split_items(L, torch.device("cpu"), xc)
-    ch, cc, coff, yb, pb = ch.numpy(), cc.numpy(), coff.numpy(), yb.numpy(), pb.numpy()
-    size = L.node_sizes()[L.half_node]
-    chi = L.edge_chi[L.half_edge]
-    for lv, halves in enumerate(topo.levels):
-        ys, ps = [], []
-        items = {}
-        for i in range(coff[lv], coff[lv + 1]):
-            items.setdefault(int(ch[i]), []).append(int(cc[i]))
-        assert set(items) == {int(h) for h in halves}
-        for h in halves:
-            P = size[h] // chi[h]
-            n = -(-P // xc)
-            assert sorted(items[int(h)]) == list(range(n))
-            ys.append((yb[h], yb[h] + size[h]))
-            ps.append((pb[h], pb[h] + n * chi[h] * chi[h]))
-        for rngs, top in ((ys, y_n), (ps, p_n)):
-            rngs.sort()
-            assert rngs[0][0] >= 0 and rngs[-1][1] <= top
-            assert all(a[1] <= b[0] for a, b in zip(rngs, rngs[1:]))
-        assert widest >= max(coff[lv + 1] - coff[lv], len(halves), int(chi[halves].sum()))
