@@ -544,10 +544,10 @@ __global__ void __launch_bounds__(GAUGE_THREADS) vidal_distance_kernel(dqz_graph
     for (int i = tid; i < ce; i += blockDim.x)
       if (Rm[i * ce + i].x > eps) Rm[i * ce + i].x -= idv;
     __syncthreads();
-    herm_eigh(Rm, ce, nullptr, ce, ce, w, rots, red);
-    double t = 0.0;
-    for (int i = tid; i < ce; i += blockDim.x) t += fabs(w[i]);
-    t = block_sum(t, red);
+    // the trace norm from the eigenvalues (tridiagonal reduction + implicit
+    // QL; the staging area is free again for its vectors)
+    const double t = herm_trace_norm(Rm, ce, ce, U, U + DQZ_MAX_CHI, reinterpret_cast<double *>(U + 2 * DQZ_MAX_CHI),
+                                     reinterpret_cast<double *>(U + 3 * DQZ_MAX_CHI), red);
     if (tid == 0) partial[h] = t;
     __syncthreads();
   }

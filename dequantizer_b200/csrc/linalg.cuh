@@ -164,6 +164,119 @@ static __device__ void herm_eigh(cd *A, int lda, cd *V, int ldv, int n, double *
   __syncthreads();
 }
 
+// Sum of |eigenvalues| (the trace norm) of a Hermitian n x n matrix A
+// (row-major, lda; destroyed), n <= 64. The eigenvalues without vectors, in
+// far fewer CTA barriers than the Jacobi forms: Householder reduction to a
+// real tridiagonal matrix (the lower-triangle steps of LAPACK's zhetd2: per
+// column k, H = I - tau v v^H from x = A[k+1:, k], x' = tau A22 v,
+// w = x' - tau^* (v^H x') v / 2, A22 -= w v^H + v w^H; five barriers a
+// column), then the eigenvalues of the tridiagonal by implicit QL with
+// Wilkinson shifts on one thread (Bowdler, Martin, Reinsch and Wilkinson,
+// Numer. Math. 11 (1968) 293-306). Scratch in shared memory: v, x (n complex
+// each), d, e (n doubles each), red (33 doubles). The input must be Hermitian
+// up to rounding (the imaginary parts of its diagonal are ignored).
+static __device__ double herm_trace_norm(cd *A, int lda, int n, cd *v, cd *x, double *d, double *e, double *red) {
+  const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
+  __shared__ cd tau_sh, scale_sh, s_sh;
+  __shared__ int skip_sh;
+  __shared__ double norm_sh;
+  for (int k = 0; k + 2 < n; ++k) {
+    const int m = n - k - 1;  // length of the column below the diagonal
+    double xn2 = 0.0;
+    for (int i = 2 + tid; i <= m; i += nt) xn2 += cabs2(A[(long long)(k + i) * lda + k]);
+    xn2 = block_sum(xn2, red);
+    if (tid == 0) {
+      const cd alpha = A[(long long)(k + 1) * lda + k];
+      int skip = xn2 == 0.0 && alpha.y == 0.0;
+      if (!skip) {
+        const double beta = -copysign(sqrt(cabs2(alpha) + xn2), alpha.x);
+        tau_sh = mk((beta - alpha.x) / beta, -alpha.y / beta);
+        scale_sh = cdiv(mk(1.0, 0.0), mk(alpha.x - beta, alpha.y));
+        A[(long long)(k + 1) * lda + k] = mk(beta, 0.0);
+      }
+      skip_sh = skip;
+    }
+    __syncthreads();
+    if (skip_sh) continue;
+    const cd tau = tau_sh, sc = scale_sh;
+    for (int i = tid; i < m; i += nt) v[i] = i == 0 ? mk(1.0, 0.0) : cmul(A[(long long)(k + 1 + i) * lda + k], sc);
+    __syncthreads();
+    // x = tau A22 v, a warp per row
+    for (int i = warp; i < m; i += nw) {
+      const cd *row = A + (long long)(k + 1 + i) * lda + (k + 1);
+      cd acc = czero();
+      for (int j = lane; j < m; j += 32) cfma(acc, row[j], v[j]);
+      acc = warp_csum(acc);
+      if (lane == 0) x[i] = cmul(tau, acc);
+    }
+    __syncthreads();
+    if (warp == 0) {  // s = v^H x
+      cd acc = czero();
+      for (int j = lane; j < m; j += 32) cfmac(acc, v[j], x[j]);
+      acc = warp_csum(acc);
+      if (lane == 0) s_sh = acc;
+    }
+    __syncthreads();
+    const cd hs = cmul(mk(0.5 * tau.x, -0.5 * tau.y), s_sh);  // tau^* s / 2
+    for (int i = tid; i < m; i += nt) x[i] = csub(x[i], cmul(hs, v[i]));
+    __syncthreads();
+    for (int idx = tid; idx < m * m; idx += nt) {
+      const int i = idx / m, j = idx - i * m;
+      cd *a = A + (long long)(k + 1 + i) * lda + (k + 1 + j);
+      *a = csub(*a, cadd(cmul(x[i], cconj(v[j])), cmul(v[i], cconj(x[j]))));
+    }
+    __syncthreads();
+  }
+  for (int i = tid; i < n; i += nt) {
+    d[i] = A[(long long)i * lda + i].x;
+    e[i] = i + 1 < n ? sqrt(cabs2(A[(long long)(i + 1) * lda + i])) : 0.0;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    const double eps = 2.220446049250313e-16;
+    for (int l = 0; l < n; ++l) {
+      for (int it = 0; it < 60; ++it) {
+        int m = l;
+        while (m < n - 1 && !(fabs(e[m]) <= eps * (fabs(d[m]) + fabs(d[m + 1])))) ++m;
+        if (m == l) break;
+        // shift from the leading 2 x 2 of the unreduced block l..m
+        double g = (d[l + 1] - d[l]) / (2.0 * e[l]);
+        double r = hypot(g, 1.0);
+        g = d[m] - d[l] + e[l] / (g + copysign(r, g));
+        double s = 1.0, c = 1.0, p = 0.0;
+        bool deflated = false;
+        for (int i = m - 1; i >= l; --i) {
+          const double f = s * e[i], b = c * e[i];
+          r = hypot(f, g);
+          e[i + 1] = r;
+          if (r == 0.0) {  // the rotation underflowed: the block splits here
+            d[i + 1] -= p;
+            e[m] = 0.0;
+            deflated = true;
+            break;
+          }
+          s = f / r;
+          c = g / r;
+          g = d[i + 1] - p;
+          r = (d[i] - g) * s + 2.0 * c * b;
+          p = s * r;
+          d[i + 1] = g + p;
+          g = c * r - b;
+        }
+        if (deflated) continue;
+        d[l] -= p;
+        e[l] = g;
+        e[m] = 0.0;
+      }
+    }
+    double t = 0.0;
+    for (int i = 0; i < n; ++i) t += fabs(d[i]);
+    norm_sh = t;
+  }
+  __syncthreads();
+  return norm_sh;
+}
+
 // One-sided Jacobi SVD on the columns of A (m x n, column-major, lda), m >= n
 // is not required but only min(m, n) columns come out non-zero when m < n.
 // On return column j of A is s_j u_j, V (n x n, column-major, ldv) holds the
