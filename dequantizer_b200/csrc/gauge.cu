@@ -459,16 +459,30 @@ __global__ void __launch_bounds__(GAUGE_THREADS) vidal_distance_kernel(dqz_graph
     for (int k = 0; k < 4; ++k)
 #pragma unroll
       for (int m = 0; m < 4; ++m) acc[k][m] = czero();
+    // 32-bit index arithmetic below 2^31 entries (64-bit division is a long
+    // instruction sequence, and the staging runs it per entry)
+    const bool small = s.size < (1ll << 31);
+    const FastDiv fRe((unsigned)(small ? Re : 1));
     for (long long x0 = 0; x0 < P; x0 += rows) {
       const int nr = (int)((P - x0) < rows ? (P - x0) : rows);
       for (int xl = tid; xl < nr; xl += GAUGE_THREADS) {
-        const long long x = x0 + xl;
-        const long long l = x / Re, r = x - l * Re;
-        const long long o0 = (l * ce) * Re + r;
         double wt = 1.0;
-        for (int f = 0; f < s.k; ++f) {
-          if (f == e) continue;
-          wt *= lam[f][(int)((o0 / s.stride[f]) % s.dims[f])];
+        if (small) {
+          const unsigned x = (unsigned)(x0 + xl);
+          const unsigned l = fRe.div(x), r = x - l * (unsigned)Re;
+          const unsigned o0 = (l * (unsigned)ce) * (unsigned)Re + r;
+          for (int f = 0; f < s.k; ++f) {
+            if (f == e) continue;
+            wt *= lam[f][(o0 / (unsigned)s.stride[f]) % (unsigned)s.dims[f]];
+          }
+        } else {
+          const long long x = x0 + xl;
+          const long long l = x / Re, r = x - l * Re;
+          const long long o0 = (l * ce) * Re + r;
+          for (int f = 0; f < s.k; ++f) {
+            if (f == e) continue;
+            wt *= lam[f][(int)((o0 / s.stride[f]) % s.dims[f])];
+          }
         }
         wrow[xl] = wt;
       }
@@ -477,9 +491,15 @@ __global__ void __launch_bounds__(GAUGE_THREADS) vidal_distance_kernel(dqz_graph
         const int xl = q % nr, a = q / nr;
         cd y = czero();
         if (a < ce) {
-          const long long x = x0 + xl;
-          const long long l = x / Re, r = x - l * Re;
-          y = cscale(T[(l * ce + a) * Re + r], wrow[xl]);
+          if (small) {
+            const unsigned x = (unsigned)(x0 + xl);
+            const unsigned l = fRe.div(x), r = x - l * (unsigned)Re;
+            y = cscale(T[(l * (unsigned)ce + (unsigned)a) * (unsigned)Re + r], wrow[xl]);
+          } else {
+            const long long x = x0 + xl;
+            const long long l = x / Re, r = x - l * Re;
+            y = cscale(T[(l * ce + a) * Re + r], wrow[xl]);
+          }
         }
         U[xl * ld + a] = y;
       }
