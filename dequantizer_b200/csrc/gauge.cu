@@ -416,7 +416,6 @@ __global__ void __launch_bounds__(GAUGE_THREADS) vidal_distance_kernel(dqz_graph
                                                                         const int32_t *__restrict__ sel, int n_sel) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double *red = reinterpret_cast<double *>(smem_raw);
-  Rot *rots = reinterpret_cast<Rot *>(smem_raw + 48 * sizeof(double));
   cd *U = reinterpret_cast<cd *>(smem_raw + round16(48 * sizeof(double) + (DQZ_MAX_CHI / 2 + 1) * sizeof(Rot)));
   size_t umax = 0;
   int rmax = 0;
@@ -426,7 +425,6 @@ __global__ void __launch_bounds__(GAUGE_THREADS) vidal_distance_kernel(dqz_graph
   }
   double *wrow = reinterpret_cast<double *>(U + umax);
   cd *Rm = reinterpret_cast<cd *>(reinterpret_cast<unsigned char *>(wrow) + round16((size_t)rmax * sizeof(double)));
-  double *w = reinterpret_cast<double *>(Rm + max_chi * max_chi);
   __shared__ cd trace_sh;
   __shared__ int count_sh;
   const int total = sel ? n_sel : g.n_halves;
