@@ -459,7 +459,7 @@ __global__ void __launch_bounds__(BP_THREADS) bp_sweep_levels_kernel(
 // once, so the level lasts as long as one item, and more threads per item
 // shorten it (two CTAs of 512 threads still fit per SM).
 constexpr int SLICED_THREADS = 512;
-__global__ void __launch_bounds__(SLICED_THREADS) bp_sweep_sliced_kernel(
+__global__ void __launch_bounds__(SLICED_THREADS, 2) bp_sweep_sliced_kernel(
     dqz_graph_t g, const cd *__restrict__ T, const cd *n2e_old, const cd *e2n_old, cd *n2e_new, cd *e2n_new,
     const uint8_t *__restrict__ src_sel, const uint8_t *__restrict__ edge_new, const int32_t *__restrict__ halves,
     const int32_t *__restrict__ level_off, const int32_t *__restrict__ item_half,
