@@ -17,7 +17,7 @@ extern "C" int dqz_set_tuning(int32_t knob, int32_t value) {
   if (knob < 0 || knob >= DQZ_TUNE_COUNT || value < 0) return DQZ_ERR_ARG;
   if ((knob == DQZ_TUNE_GAUGE_EDGE_WARPS || knob == DQZ_TUNE_GAUGE_DIST_WARPS) && value > 8) return DQZ_ERR_ARG;
   if (knob == DQZ_TUNE_GAUGE_PATH && value > 2) return DQZ_ERR_ARG;
-  if (knob == DQZ_TUNE_SU_ONCHIP && value > 3) return DQZ_ERR_ARG;
+  if (knob == DQZ_TUNE_SU_ONCHIP && value > 4) return DQZ_ERR_ARG;
   if (knob == DQZ_TUNE_SWEEP_ONECTA && value > 2) return DQZ_ERR_ARG;
   g_tuning[knob] = value;
   return DQZ_OK;

@@ -431,7 +431,8 @@ size_t su_smem_bytes(int max_cols) {
 constexpr int SUF_THREADS = 512;
 constexpr size_t SUF_SMEM_MAX = 220 * 1024;  // dynamic shared memory per CTA (plus ~2.3 KB static)
 
-__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(SUF_THREADS, 1)
+template <int THREADS, int MIN_BLOCKS>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(THREADS, MIN_BLOCKS)
     simple_update_onchip_kernel(dqz_graph_t g, cd *Tall, double *lambdas, const int32_t *edges,
                                 const uint8_t *ctrl_first, const cd *halves, const int32_t *ranks, int n, double eps,
                                 int max_rank, double *err_out, double *ent_out, long long cap, uint8_t *done,
@@ -767,7 +768,7 @@ __host__ __device__ inline size_t su_marks_bytes(int32_t n) { return ((size_t)n 
 // SU_CLUSTER_PAIRS jobs in flight (one CTA per SM), each CTA's slice bounded
 // by the side's need for matrices of max_rows x max_cols (B and S at most
 // max_rows x max_cols each, core / W / X at most 3 max_cols^2 beyond that).
-constexpr int SU_CLUSTER_PAIRS = 74;
+constexpr int SU_CLUSTER_PAIRS = 148;
 __host__ __device__ inline long long su_cluster_cap(int max_rows, int max_cols) {
   return suf_even(2ll * max_rows * max_cols + 3ll * max_cols * max_cols + 8ll * max_cols + 64);
 }
@@ -812,17 +813,28 @@ extern "C" int dqz_simple_update(const dqz_graph_t *g, void *tensors, double *la
   // 2 = the cluster forms at any batch size, 3 = no global-workspace form.
   const int knob = dqz_get_tuning(DQZ_TUNE_SU_ONCHIP);
   const int pairs = n < sms / 2 ? n : sms / 2;  // one CTA per SM, two per cluster
-  if (max_rows >= SUF_MIN_ROWS && (n <= sms || knob == 2) && knob != 1) {
-    DQZ_SMEM_ATTR_ONCE(simple_update_onchip_kernel, SUF_SMEM_MAX);
+  if (max_rows >= SUF_MIN_ROWS && knob == 4) {
+    // every 256-row job on the global-workspace cluster form, 256 threads a
+    // CTA and two clusters per SM pair
+    auto *gws = simple_update_onchip_kernel<256, 2>;
+    marks = static_cast<uint8_t *>(scratch);
+    const int cp = su_cluster_pairs(n) < sms ? su_cluster_pairs(n) : sms;
+    gws<<<2 * cp, 256, 0, stream>>>(*g, (cd *)tensors, lambdas, edges, ctrl_is_first, (const cd *)halves, ranks, n,
+                                    eps, max_rank, err, entropy, su_cluster_cap(max_rows, max_cols), marks,
+                                    job_scratch, 0);
+    DQZ_CHECK_LAUNCH();
+  } else if (max_rows >= SUF_MIN_ROWS && (n <= sms || knob == 2) && knob != 1) {
+    auto *onchip = simple_update_onchip_kernel<SUF_THREADS, 1>;
+    DQZ_SMEM_ATTR_ONCE(onchip, SUF_SMEM_MAX);
     const long long cap = (long long)(SUF_SMEM_MAX / sizeof(cd));
     marks = static_cast<uint8_t *>(scratch);
-    simple_update_onchip_kernel<<<2 * pairs, SUF_THREADS, SUF_SMEM_MAX, stream>>>(
+    onchip<<<2 * pairs, SUF_THREADS, SUF_SMEM_MAX, stream>>>(
         *g, (cd *)tensors, lambdas, edges, ctrl_is_first, (const cd *)halves, ranks, n, eps, max_rank, err, entropy,
         cap, marks, nullptr, 0);
     DQZ_CHECK_LAUNCH();
     if (knob != 3) {
       const int cp = su_cluster_pairs(n) < pairs ? su_cluster_pairs(n) : pairs;
-      simple_update_onchip_kernel<<<2 * cp, SUF_THREADS, 0, stream>>>(
+      onchip<<<2 * cp, SUF_THREADS, 0, stream>>>(
           *g, (cd *)tensors, lambdas, edges, ctrl_is_first, (const cd *)halves, ranks, n, eps, max_rank, err,
           entropy, su_cluster_cap(max_rows, max_cols), marks, job_scratch, 1);
       DQZ_CHECK_LAUNCH();

@@ -80,7 +80,8 @@ int dqz_device_supported(int device); /* 1 when the device is sm_100 */
 #define DQZ_TUNE_SU_GRID 3          /* CTAs of simple_update (>= 1), jobs loop over the grid     */
 #define DQZ_TUNE_SU_ONCHIP 4        /* simple update: 1 = one-CTA global-scratch kernel only,
                                        2 = cluster forms at any batch size, 3 = no global-workspace
-                                       cluster form                                               */
+                                       cluster form, 4 = the global-workspace cluster form (256
+                                       threads) for every job with 256+ rows                      */
 #define DQZ_TUNE_SWEEP_ONECTA 5     /* asynchronous one-launch sweep in one CTA: 1 = never,
                                        2 = wherever its warps' buffers fit                     */
 #define DQZ_TUNE_COUNT 6

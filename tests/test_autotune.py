@@ -22,7 +22,7 @@ def test_knobs_roundtrip_and_validation():
            "sweep_onecta": 2}
     autotune.set_knobs(cfg)
     assert autotune.get_knobs() == cfg
-    assert lib.dqz_set_tuning(autotune.KNOBS["su_onchip"], 4) == _lib.DQZ_ERR_ARG
+    assert lib.dqz_set_tuning(autotune.KNOBS["su_onchip"], 5) == _lib.DQZ_ERR_ARG
     assert lib.dqz_set_tuning(autotune.KNOBS["sweep_onecta"], 3) == _lib.DQZ_ERR_ARG
     assert lib.dqz_set_tuning(autotune.KNOBS["gauge_edge_warps"], 9) == _lib.DQZ_ERR_ARG
     assert lib.dqz_set_tuning(autotune.KNOBS["gauge_path"], 3) == _lib.DQZ_ERR_ARG

@@ -236,7 +236,8 @@ def test_simple_update_forms_agree_on_a_batch(chi, nn):
     than SMs) and of bond-32 jobs (2048 x 64 per side, above shared memory)
     through each form the knob selects: the one-CTA global-scratch kernel
     (su_onchip = 1), the cluster forms at any batch size (2), the default rule
-    (0) and the default without the global-workspace cluster form (3). Lambdas,
+    (0), the default without the global-workspace cluster form (3) and the
+    global-workspace cluster form with 256 threads for every job (4). Lambdas,
     truncation errors and entropies agree to 1e-12, and the two-site tensors
     around the updated bonds (gauge-invariant) to 1e-10 relative."""
     from dequantizer_b200 import _lib, autotune
@@ -271,7 +272,7 @@ def test_simple_update_forms_agree_on_a_batch(chi, nn):
     rk = torch.from_numpy(ranks).to(dev)
     out = {}
     try:
-        for knob in (1, 2, 0, 3):
+        for knob in (1, 2, 0, 3, 4):
             autotune.set_knobs({"su_onchip": knob})
             T, lam = T0.clone(), lam0.clone()
             err = torch.empty(n, dtype=torch.float64, device=dev)
@@ -288,7 +289,7 @@ def test_simple_update_forms_agree_on_a_batch(chi, nn):
     finally:
         autotune.set_knobs({"su_onchip": 0})
     ref = out[1]
-    for knob in (2, 0, 3):
+    for knob in (2, 0, 3, 4):
         T, lam, err, ent = out[knob]
         assert float((lam - ref[1]).abs().max()) < 1e-12
         assert float((err - ref[2]).abs().max()) < 1e-12
