@@ -356,11 +356,12 @@ int dqz_apply_half_gates(const void *tensors_in, void *tensors_out, const int64_
  * Writes Gamma tensors in place (capacity layout), lambdas, edge_chi, and
  * err/entropy per job. max_rows / max_cols bound the rows (d x the other
  * bonds) and columns (bond x gate rank) of the jobs' matrices.
- * In batches of at most one job per SM, jobs with a 256-row matrix or more run
- * on a cluster form (two CTAs per job, one per side, a two-step QR: lower
- * latency) with their matrices in shared memory where they fit, else in a
- * global workspace inside `scratch`; the others on a one-CTA kernel with its
- * matrices in `scratch`. The scratch (dqz_simple_update_scratch_bytes) also
+ * Jobs with a 256-row matrix or more run on a cluster form (two CTAs per job,
+ * one per side, a two-step QR): in batches of at most one job per SM with
+ * their matrices in shared memory where they fit, else in a global workspace
+ * inside `scratch`; in larger batches all in the global workspace (256
+ * threads a CTA); the others on a one-CTA kernel with its matrices in
+ * `scratch`. The scratch (dqz_simple_update_scratch_bytes) also
  * holds one byte per job recording which form did it. Knob
  * DQZ_TUNE_SU_ONCHIP: 1 sends every job to the one-CTA kernel, 2 uses the
  * cluster forms at any batch size, 3 keeps the global-workspace cluster form
