@@ -65,6 +65,47 @@ __device__ __forceinline__ bool jacobi_rot(double a, double b, cd c, Rot &r) {
   return true;
 }
 
+// One Jacobi step's update A <- J^H A J on the 2 x 2 blocks of the step's
+// index pairs (rows of pair P, columns of pair Q): each entry gets the column
+// rotation of its column pair and then the row rotation of its row pair,
+// exactly as a column pass followed by a row pass would apply them, but in one
+// pass over A (one barrier less a step). Pairs are those of rr_pair; a pair's
+// second index may be the padding index n (never rotated).
+__device__ __forceinline__ void jacobi_block_update(cd *A, int lda, int n, int np, int step, const Rot *rots, int P,
+                                                    int Q) {
+  int p1, q1, p2, q2;
+  rr_pair(step, P, np, p1, q1);
+  rr_pair(step, Q, np, p2, q2);
+  const Rot &r1 = rots[P], &r2 = rots[Q];
+  const bool rot1 = r1.p >= 0, rot2 = r2.p >= 0;
+  if (!rot1 && !rot2) return;
+  const bool v1 = q1 < n, v2 = q2 < n;
+  cd b00 = A[p1 * lda + p2];
+  cd b01 = v2 ? A[p1 * lda + q2] : czero();
+  cd b10 = v1 ? A[q1 * lda + p2] : czero();
+  cd b11 = (v1 && v2) ? A[q1 * lda + q2] : czero();
+  if (rot2) {  // columns (p2, q2): A J
+    const cd n00 = cadd(cmul(b00, r2.j00), cmul(b01, r2.j10)), n01 = cadd(cmul(b00, r2.j01), cmul(b01, r2.j11));
+    const cd n10 = cadd(cmul(b10, r2.j00), cmul(b11, r2.j10)), n11 = cadd(cmul(b10, r2.j01), cmul(b11, r2.j11));
+    b00 = n00;
+    b01 = n01;
+    b10 = n10;
+    b11 = n11;
+  }
+  if (rot1) {  // rows (p1, q1): J^H A
+    const cd n00 = cadd(cmulc(r1.j00, b00), cmulc(r1.j10, b10)), n10 = cadd(cmulc(r1.j01, b00), cmulc(r1.j11, b10));
+    const cd n01 = cadd(cmulc(r1.j00, b01), cmulc(r1.j10, b11)), n11 = cadd(cmulc(r1.j01, b01), cmulc(r1.j11, b11));
+    b00 = n00;
+    b01 = n01;
+    b10 = n10;
+    b11 = n11;
+  }
+  A[p1 * lda + p2] = b00;
+  if (v2) A[p1 * lda + q2] = b01;
+  if (v1) A[q1 * lda + p2] = b10;
+  if (v1 && v2) A[q1 * lda + q2] = b11;
+}
+
 // Hermitian eigendecomposition. A (n x n, row-major, lda) is destroyed; on
 // return w[i] holds eigenvalue i and column i of V (row-major, ldv) the
 // matching eigenvector (unsorted); V may be null (eigenvalues only, the same
@@ -129,31 +170,18 @@ static __device__ void herm_eigh(cd *A, int lda, cd *V, int ldv, int n, double *
           rots[i] = r;
         }
         __syncthreads();
-        // A <- A J and V <- V J on columns (p, q)
-        for (int idx = tid; idx < npairs * n; idx += nt) {
-          const Rot &r = rots[idx / n];
-          if (r.p < 0) continue;
-          int row = idx % n;
-          cd x = A[row * lda + r.p], y = A[row * lda + r.q];
-          A[row * lda + r.p] = cadd(cmul(x, r.j00), cmul(y, r.j10));
-          A[row * lda + r.q] = cadd(cmul(x, r.j01), cmul(y, r.j11));
-          if (V) {
-            x = V[row * ldv + r.p];
-            y = V[row * ldv + r.q];
+        // A <- J^H A J by 2 x 2 blocks, V <- V J on columns (p, q)
+        for (int blk = tid; blk < npairs * npairs; blk += nt)
+          jacobi_block_update(A, lda, n, np, step, rots, blk / npairs, blk % npairs);
+        if (V)
+          for (int idx = tid; idx < npairs * n; idx += nt) {
+            const Rot &r = rots[idx / n];
+            if (r.p < 0) continue;
+            const int row = idx % n;
+            const cd x = V[row * ldv + r.p], y = V[row * ldv + r.q];
             V[row * ldv + r.p] = cadd(cmul(x, r.j00), cmul(y, r.j10));
             V[row * ldv + r.q] = cadd(cmul(x, r.j01), cmul(y, r.j11));
           }
-        }
-        __syncthreads();
-        // A <- J^H A on rows (p, q)
-        for (int idx = tid; idx < npairs * n; idx += nt) {
-          const Rot &r = rots[idx / n];
-          if (r.p < 0) continue;
-          int col = idx % n;
-          cd x = A[r.p * lda + col], y = A[r.q * lda + col];
-          A[r.p * lda + col] = cadd(cmulc(r.j00, x), cmulc(r.j10, y));
-          A[r.q * lda + col] = cadd(cmulc(r.j01, x), cmulc(r.j11, y));
-        }
         __syncthreads();
       }
       if (!rotated_sh) break;
@@ -626,29 +654,17 @@ static __device__ void warp_herm_eigh(cd *A, int lda, cd *V, int ldv, int n, dou
           rots[lane] = r;
         }
         __syncwarp();
-        for (int idx = lane; idx < npairs * n; idx += 32) {
-          const Rot &r = rots[idx / n];
-          if (r.p < 0) continue;
-          int row = idx % n;
-          cd x = A[row * lda + r.p], y = A[row * lda + r.q];
-          A[row * lda + r.p] = cadd(cmul(x, r.j00), cmul(y, r.j10));
-          A[row * lda + r.q] = cadd(cmul(x, r.j01), cmul(y, r.j11));
-          if (V) {
-            x = V[row * ldv + r.p];
-            y = V[row * ldv + r.q];
+        for (int blk = lane; blk < npairs * npairs; blk += 32)
+          jacobi_block_update(A, lda, n, np, step, rots, blk / npairs, blk % npairs);
+        if (V)
+          for (int idx = lane; idx < npairs * n; idx += 32) {
+            const Rot &r = rots[idx / n];
+            if (r.p < 0) continue;
+            const int row = idx % n;
+            const cd x = V[row * ldv + r.p], y = V[row * ldv + r.q];
             V[row * ldv + r.p] = cadd(cmul(x, r.j00), cmul(y, r.j10));
             V[row * ldv + r.q] = cadd(cmul(x, r.j01), cmul(y, r.j11));
           }
-        }
-        __syncwarp();
-        for (int idx = lane; idx < npairs * n; idx += 32) {
-          const Rot &r = rots[idx / n];
-          if (r.p < 0) continue;
-          int col = idx % n;
-          cd x = A[r.p * lda + col], y = A[r.q * lda + col];
-          A[r.p * lda + col] = cadd(cmulc(r.j00, x), cmulc(r.j10, y));
-          A[r.q * lda + col] = cadd(cmulc(r.j01, x), cmulc(r.j11, y));
-        }
         __syncwarp();
       }
       if (!__any_sync(0xffffffffu, rotated)) break;
