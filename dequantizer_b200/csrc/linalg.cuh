@@ -322,38 +322,50 @@ static __device__ void hestenes(cd *A, int lda, int m, int n, cd *V, int ldv, do
   double fro = 0.0;
   for (int i = tid; i < m * n; i += nt) fro += cabs2(A[(long long)(i / m) * lda + (i % m)]);
   const double null_thr = hestenes_null_scale(m) * block_sum(fro, red);
+  // With more pairs per round than warps, each 16-lane half of a warp takes a
+  // pair, so a warp's two pairs run side by side instead of one after the other.
+  const bool half = npairs > nw;
+  const int hw = half ? lane >> 4 : 0, hl = half ? lane & 15 : lane, ls = half ? 16 : 32, per = half ? 2 : 1;
   if (n > 1) {
     for (int sweep = 0; sweep < max_sweeps; ++sweep) {
       if (tid == 0) *flag = 0;
       __syncthreads();
       for (int step = 0; step < np - 1; ++step) {
-        for (int i = warp; i < npairs; i += nw) {
-          int p, q;
-          rr_pair(step, i, np, p, q);
-          if (q >= n) continue;
-          cd *ap = A + (long long)p * lda, *aq = A + (long long)q * lda;
+        for (int ib = warp * per; ib < npairs; ib += nw * per) {  // warp-uniform trip count
+          const int i = ib + hw;
+          int p = 0, q = n;
+          if (i < npairs) rr_pair(step, i, np, p, q);
+          const bool live = q < n;
+          cd *ap = A + (long long)p * lda, *aq = A + (long long)(live ? q : p) * lda;
           double al = 0.0, be = 0.0;
           cd ga = czero();
-          for (int r = lane; r < m; r += 32) {
-            cd x = ap[r], y = aq[r];
-            al += cabs2(x);
-            be += cabs2(y);
-            cfmac(ga, x, y);
+          if (live)
+            for (int r = hl; r < m; r += ls) {
+              cd x = ap[r], y = aq[r];
+              al += cabs2(x);
+              be += cabs2(y);
+              cfmac(ga, x, y);
+            }
+          if (half) {
+            al = half_sum(al);
+            be = half_sum(be);
+            ga = mk(half_sum(ga.x), half_sum(ga.y));
+          } else {
+            al = warp_sum(al);
+            be = warp_sum(be);
+            ga = warp_csum(ga);
           }
-          al = warp_sum(al);
-          be = warp_sum(be);
-          ga = warp_csum(ga);
-          if (!(al > null_thr) || !(be > null_thr) || !(cabs2(ga) > tol * tol * al * be)) continue;
+          if (!live || !(al > null_thr) || !(be > null_thr) || !(cabs2(ga) > tol * tol * al * be)) continue;
           Rot r;
           if (!jacobi_rot(al, be, ga, r)) continue;
-          if (lane == 0) *flag = 1;
-          for (int k = lane; k < m; k += 32) {
+          if (hl == 0) *flag = 1;
+          for (int k = hl; k < m; k += ls) {
             cd x = ap[k], y = aq[k];
             ap[k] = cadd(cmul(x, r.j00), cmul(y, r.j10));
             aq[k] = cadd(cmul(x, r.j01), cmul(y, r.j11));
           }
           cd *vp = V + (long long)p * ldv, *vq = V + (long long)q * ldv;
-          for (int k = lane; k < n; k += 32) {
+          for (int k = hl; k < n; k += ls) {
             cd x = vp[k], y = vq[k];
             vp[k] = cadd(cmul(x, r.j00), cmul(y, r.j10));
             vq[k] = cadd(cmul(x, r.j01), cmul(y, r.j11));
