@@ -699,37 +699,49 @@ static __device__ void warp_hestenes(cd *A, int lda, int m, int n, cd *V, int ld
   for (int i = lane; i < m * n; i += 32) fro += cabs2(A[(long long)(i / m) * lda + (i % m)]);
   const double null_thr = hestenes_null_scale(m) * warp_sum(fro);
   __syncwarp();
+  // lpp consecutive lanes share a column pair (rows strided by lpp, sums over
+  // the group by xor shuffles): all 32 lanes work when a round has few pairs.
+  int lpp = 32;
+  while (lpp > 1 && lpp * npairs > 32) lpp >>= 1;
+  const int grp = lane / lpp, sub = lane % lpp, ppass = 32 / lpp;
   if (n > 1) {
     for (int sweep = 0; sweep < max_sweeps; ++sweep) {
       bool rotated = false;
       for (int step = 0; step < np - 1; ++step) {
-        if (lane < npairs) {
-          int p, q;
-          rr_pair(step, lane, np, p, q);
-          if (q < n) {
-            cd *ap = A + (long long)p * lda, *aq = A + (long long)q * lda;
-            double al = 0.0, be = 0.0;
-            cd ga = czero();
-            for (int r = 0; r < m; ++r) {
+        for (int i0 = 0; i0 < npairs; i0 += ppass) {  // warp-uniform trip count
+          const int i = i0 + grp;
+          int p = 0, q = n;
+          if (i < npairs) rr_pair(step, i, np, p, q);
+          const bool live = q < n;
+          cd *ap = A + (long long)p * lda, *aq = A + (long long)(live ? q : p) * lda;
+          double al = 0.0, be = 0.0;
+          cd ga = czero();
+          if (live)
+            for (int r = sub; r < m; r += lpp) {
               cd x = ap[r], y = aq[r];
               al += cabs2(x);
               be += cabs2(y);
               cfmac(ga, x, y);
             }
-            Rot rt;
-            if (al > null_thr && be > null_thr && cabs2(ga) > tol * tol * al * be && jacobi_rot(al, be, ga, rt)) {
-              rotated = true;
-              for (int k = 0; k < m; ++k) {
-                cd x = ap[k], y = aq[k];
-                ap[k] = cadd(cmul(x, rt.j00), cmul(y, rt.j10));
-                aq[k] = cadd(cmul(x, rt.j01), cmul(y, rt.j11));
-              }
-              cd *vp = V + (long long)p * ldv, *vq = V + (long long)q * ldv;
-              for (int k = 0; k < n; ++k) {
-                cd x = vp[k], y = vq[k];
-                vp[k] = cadd(cmul(x, rt.j00), cmul(y, rt.j10));
-                vq[k] = cadd(cmul(x, rt.j01), cmul(y, rt.j11));
-              }
+          for (int o = lpp >> 1; o > 0; o >>= 1) {
+            al += __shfl_xor_sync(0xffffffffu, al, o);
+            be += __shfl_xor_sync(0xffffffffu, be, o);
+            ga.x += __shfl_xor_sync(0xffffffffu, ga.x, o);
+            ga.y += __shfl_xor_sync(0xffffffffu, ga.y, o);
+          }
+          Rot rt;
+          if (live && al > null_thr && be > null_thr && cabs2(ga) > tol * tol * al * be && jacobi_rot(al, be, ga, rt)) {
+            rotated = true;
+            for (int k = sub; k < m; k += lpp) {
+              cd x = ap[k], y = aq[k];
+              ap[k] = cadd(cmul(x, rt.j00), cmul(y, rt.j10));
+              aq[k] = cadd(cmul(x, rt.j01), cmul(y, rt.j11));
+            }
+            cd *vp = V + (long long)p * ldv, *vq = V + (long long)q * ldv;
+            for (int k = sub; k < n; k += lpp) {
+              cd x = vp[k], y = vq[k];
+              vp[k] = cadd(cmul(x, rt.j00), cmul(y, rt.j10));
+              vq[k] = cadd(cmul(x, rt.j01), cmul(y, rt.j11));
             }
           }
         }
