@@ -91,6 +91,10 @@ class BatchedAnnealer:
         self.bf16_sweeps: List[List[int]] = []
         self.fp32_sweeps: List[List[int]] = []
         self.vd_checks: List[List[int]] = []
+        # per instance, from its previous regauge in the mixed form: FP64 sweeps
+        # to the accuracy and the distance's geometric rate per sweep there
+        self._prev_iters: Optional[np.ndarray] = None
+        self._prev_rate: Optional[np.ndarray] = None
         if not torch.cuda.is_available():
             raise RuntimeError("BatchedAnnealer runs on the GPU only")
         _lib.lib()
@@ -254,6 +258,9 @@ class BatchedAnnealer:
                 n2e, e2n = self._bf16_prephase(T, n2e, e2n, todo)
         lazy = self.precision == "mixed"
         next_check = np.ones(self.n_inst, dtype=np.int64)
+        if lazy and self._prev_iters is not None:
+            # first check two sweeps before where the previous regauge got there
+            next_check = np.maximum(1, self._prev_iters - 2)
         hist: List[List] = [[] for _ in range(self.n_inst)]
         checks = np.zeros(self.n_inst, dtype=np.int64)
         while True:
@@ -289,16 +296,34 @@ class BatchedAnnealer:
             if lazy:
                 for k in np.nonzero(due)[0]:
                     hist[k].append((int(iters[k]), float(vd_h[k])))
-                    next_check[k] = iters[k] + self._sweeps_to_accuracy(hist[k])
+                    prev = float(self._prev_rate[k]) if self._prev_rate is not None else float("nan")
+                    next_check[k] = iters[k] + self._sweeps_to_accuracy(hist[k], prev)
+        if lazy:
+            rate = np.full(self.n_inst, np.nan) if self._prev_rate is None else self._prev_rate.copy()
+            for k in range(self.n_inst):
+                if len(hist[k]) >= 2:
+                    (i1, v1), (i2, v2) = hist[k][-2], hist[k][-1]
+                    if 0.0 < v2 < v1 and i2 > i1:
+                        rate[k] = (v2 / v1) ** (1.0 / (i2 - i1))
+            self._prev_rate = rate
+            self._prev_iters = np.where(iters > 0, iters, self._prev_iters if self._prev_iters is not None else 0)
         self.bp_iterations.append(iters.tolist())
         self.vd_checks.append(checks.tolist())
         self.vidal_distances.append(vd_h.copy())
         return G, lam
 
-    def _sweeps_to_accuracy(self, hist, max_gap: int = 8) -> int:
+    def _sweeps_to_accuracy(self, hist, prev_rate: float = float("nan"), max_gap: int = 8) -> int:
         """FP64 sweeps until the next distance check of the mixed form: the
-        geometric rate of the last two checks extrapolated to the accuracy
-        (1 while fewer than two checks or no decrease, at most ``max_gap``)."""
+        geometric rate of the last two checks extrapolated to the accuracy (at
+        most ``max_gap``); after a single check, the rate the instance had at
+        its previous regauge (``prev_rate``, at most ``max_gap // 2``); 1 when
+        neither is known or the distance does not decrease."""
+        if len(hist) == 1:
+            v1 = hist[0][1]
+            if not (0.0 < prev_rate < 1.0) or not (v1 > self.accuracy):
+                return 1
+            k = math.ceil(math.log(self.accuracy / v1) / math.log(prev_rate))
+            return int(min(max(k, 1), max_gap // 2))
         if len(hist) < 2:
             return 1
         (i1, v1), (i2, v2) = hist[-2], hist[-1]

@@ -258,3 +258,25 @@ def test_sweep_plan_matches_layout_tables(make):
             off = L.half_msg_off[hf] if sel == _lib.SRC_E2N_OLD else L.half_msg_off[L.half_twin[hf]]
             assert row[5 + _lib.MAX_DEGREE + slot] == off * 4 + sel
             slot += 1
+
+
+def test_mixed_annealer_check_schedule():
+    """Distance-check spacing of the mixed annealer's lazy loop: two checks
+    extrapolate their geometric rate to the accuracy (at most 8 sweeps); one
+    check uses the rate of the instance's previous regauge (at most 4); no
+    usable rate or no decrease means the next sweep."""
+    from types import SimpleNamespace
+
+    from dequantizer_b200.annealing import BatchedAnnealer
+
+    f = BatchedAnnealer._sweeps_to_accuracy
+    a = SimpleNamespace(accuracy=1e-5)
+    assert f(a, []) == 1
+    assert f(a, [(3, 1e-3)]) == 1  # no previous rate
+    assert f(a, [(3, 1e-3)], 0.5) == 4  # 1e-3 * 0.5^7 < 1e-5, capped at 4
+    assert f(a, [(3, 4e-5)], 0.5) == 2  # 4e-5 * 0.5^2 = 1e-5
+    assert f(a, [(3, 1e-6)], 0.5) == 1  # already at the accuracy
+    assert f(a, [(3, 1e-3)], 1.5) == 1  # not a decrease
+    assert f(a, [(1, 1e-3), (2, 5e-4)]) == 6  # 5e-4 * 0.5^6 < 1e-5 <= 5e-4 * 0.5^5
+    assert f(a, [(1, 1e-1), (2, 5e-2)]) == 8  # capped
+    assert f(a, [(1, 1e-3), (2, 2e-3)]) == 1
