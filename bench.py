@@ -504,7 +504,10 @@ def workload_suite(args):
       every bond is at 16), FP64 and mixed precision, instance-steps/s;
       the densities of both forms after the timed steps compared;
     * eagle -- the 127-qubit kicked-Ising run's first Trotter steps (bonds
-      growing towards 32), Trotter steps/s."""
+      growing towards 32), Trotter steps/s;
+    * grad -- the annealing-schedule gradient's first Trotter steps (512-node
+      3-regular graph, J = +-1, chi 16, dt 0.1, s_t = (t + 1/2) / 200,
+      checkpoints every 10): forward and gradient seconds."""
     import torch
 
     from dequantizer_b200.annealing import BatchedAnnealer
@@ -569,6 +572,27 @@ def workload_suite(args):
     out["eagle"] = {"unit": "Trotter steps/s", "value": n_eagle / dt, "steps": n_eagle,
                     "max_bond": int(em._layout.edge_chi.max()),
                     "sample": f"the first {n_eagle} of the 20 steps (bonds growing towards 32)"}
+    del em
+    torch.cuda.empty_cache()
+    # ---- annealing-schedule gradient (config 5), first steps
+    n_grad = args.suite_grad_steps
+    if n_grad > 0:
+        from dequantizer_b200.anneal_grad import AnnealingGradient
+
+        try:
+            ag = AnnealingGradient(random_regular_energy(512, 3, seed=500, field_std=0.0), max_chi=16, dt=0.1,
+                                   checkpoint_every=10, bp_tol=1e-12)
+            s_sched = (np.arange(n_grad) + 0.5) / 200
+            E_fwd, t_fwd = _events_time(lambda: ag.energy_value(s_sched))
+            (E, grad), t_grad = _events_time(lambda: ag.value_and_grad(s_sched))
+            out["grad"] = {"unit": "s", "forward_s": t_fwd, "gradient_s": t_grad,
+                           "gradient_over_forward": t_grad / t_fwd, "steps": n_grad,
+                           "energy_matches_forward": abs(E - E_fwd) < 1e-12 * max(1.0, abs(E)),
+                           "grad_norm": float(np.linalg.norm(grad)),
+                           "sample": f"the first {n_grad} of the 200 steps (dt 0.1, s_t = (t + 1/2) / 200), "
+                                     "512 nodes, chi 16, checkpoints every 10"}
+        except Exception as exc:  # reported, not raised: the headline line still prints
+            out["grad"] = {"error": f"{type(exc).__name__}: {exc}"}
     return out
 
 
@@ -972,6 +996,8 @@ def main():
     ap.add_argument("--suite-anneal-steps", type=int, default=4)
     ap.add_argument("--suite-anneal-warm-dt", type=float, default=1.0)
     ap.add_argument("--suite-eagle-steps", type=int, default=6)
+    ap.add_argument("--suite-grad-steps", type=int, default=20,
+                    help="Trotter steps of the suite's gradient sample (0 skips it)")
     ap.add_argument("--e2e-chunks", type=int, default=8,
                     help="node ranges the end-to-end sweep streams its host inputs in (1: no overlap)")
     ap.add_argument("--no-accuracy", action="store_true")
